@@ -1,0 +1,170 @@
+/*
+ * lbm_ddf.h — C ABI of the B200 double-distribution lattice Boltzmann engine
+ * for 3D Rayleigh–Bénard convection (D3Q27 velocity populations f, D3Q27
+ * temperature populations g).
+ *
+ * It replaces the single-GPU run surface of Summer536/LBM_DDF src/:
+ *   - the compile-time fields of src/parameters.h:5-31      -> lbm_params
+ *   - the derived globals of src/globals.cu:13-23            -> lbm_derive
+ *   - initialize() / init_arrays, src/initial.cu:3-241       -> lbm_create,
+ *     lbm_init_rest, lbm_init_conduction
+ *   - the restart reader, src/initial.cu:110-205             -> lbm_load_ref_state
+ *   - the six launches and two copies of one step,
+ *     src/main.cu:27-46                                      -> lbm_step
+ *   - output_nu / diag_flow / output_profile / output_flow /
+ *     output_fg, src/output.cu:3-419 (src/rb3d.h:64-68)      -> lbm_get_observables,
+ *     lbm_get_profile, lbm_store_ref_state
+ *
+ * Conventions, unlike the reference's exit(EXIT_FAILURE) on any error
+ * (src/rb3d.h:71-79): every call returns an int status, LBM_OK (0) or a
+ * negative LBM_ERR_*; lbm_last_error() gives a message for the calling
+ * thread.  Cases are opaque handles owned by the library.  Host buffers are
+ * owned by the caller.  `stream` arguments are cudaStream_t values (NULL is
+ * the legacy default stream); calls that return host data synchronise that
+ * stream.  One case must not be used from two host threads at once.
+ *
+ * Axes and layout follow the reference: x fastest, then y, then z; node
+ * idx = (iz*LY + iy)*LX + ix; population ip of a reference-layout array at
+ * ip*N + idx; y is vertical with the hot plate below iy = 0 and the cold
+ * plate above iy = LY-1 (halfway walls).
+ */
+#ifndef LBM_DDF_H
+#define LBM_DDF_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_DDF_ABI_VERSION 1
+
+/* status codes */
+#define LBM_OK 0
+#define LBM_ERR_ARG (-1)       /* bad argument or unsupported combination */
+#define LBM_ERR_CUDA (-2)      /* a CUDA runtime call failed */
+#define LBM_ERR_NOMEM (-3)     /* device or host allocation failed */
+#define LBM_ERR_DIVERGED (-4)  /* NaN/Inf found in the state */
+#define LBM_ERR_STATE (-5)     /* call not valid in the case's current state */
+
+/* side walls (x and z faces) */
+#define LBM_SIDES_WALL 0       /* closed box: no-slip, adiabatic (reference src/streaming.cu:59-124,183-250) */
+#define LBM_SIDES_PERIODIC 1   /* x and z periodic; only the y plates are walls */
+
+/* population storage in HBM; arithmetic is FP64 for F64 and FP32 otherwise */
+#define LBM_STORE_F64 0
+#define LBM_STORE_F32 1
+#define LBM_STORE_F16S 2       /* FP16 of f_i/w_i and g_i/w_i - t0 */
+#define LBM_STORE_BF16S 3      /* BF16 of the same shifted values */
+
+/* Run surface of src/parameters.h:8-26 plus the engine's own choices. */
+typedef struct lbm_params {
+    int32_t lx, ly, lz;        /* LX, LY, LZ (>= 2, 3, 2); y vertical */
+    int32_t sides;             /* LBM_SIDES_* */
+    int32_t storage;           /* LBM_STORE_* */
+    int32_t device;            /* CUDA device ordinal */
+    double rayleigh;           /* RAYLEIGH */
+    double prandtl;            /* PRANDTL */
+    double t_hot, t_cold;      /* T_HOT, T_COLD */
+    double gravity, beta;      /* GRAVITY, BETA */
+} lbm_params;
+
+/* Derived parameters, src/globals.cu:13-23. */
+typedef struct lbm_derived {
+    double visc;               /* LY*sqrt(g*beta*dT*LY*Pr/Ra) */
+    double tau;                /* 3*visc + 0.5 */
+    double u0;                 /* sqrt(g*beta*dT*LY), free-fall velocity */
+    double diff;               /* visc / Pr */
+    double tauc;               /* 3*diff + 0.5 */
+    double t0;                 /* (T_hot + T_cold) / 2 */
+} lbm_derived;
+
+/* Observables of the macroscopic fields at the current step.  u is the
+ * reference's stored velocity sum(c f) + F/2 (src/macrovar.cu:28-30). */
+typedef struct lbm_observables {
+    int64_t step;              /* steps taken since the state was set */
+    double nu_bulk;            /* 1 + <u_y T> LY / (kappa dT)      src/output.cu:228-233 */
+    double nu_top, nu_bottom;  /* -<dT/dy>_plate LY / dT          src/output.cu:236-256 */
+    double ke;                 /* 0.5 <|u|^2> */
+    double re;                 /* sqrt(<|u|^2>) LY / visc */
+    double ux_mean, uy_mean, uz_mean, phi_mean;  /* src/output.cu:24-34 */
+    int32_t diverged;          /* 1 if any node had a NaN/Inf moment */
+    int32_t reserved;
+} lbm_observables;
+
+typedef struct lbm_case lbm_case;
+
+/* Message of the last failing call on this host thread ("" if none). */
+const char *lbm_last_error(void);
+int lbm_abi_version(void);
+
+/* src/globals.cu:13-23.  Fails with LBM_ERR_ARG for a bad grid or parameters. */
+int lbm_derive(const lbm_params *p, lbm_derived *out);
+
+/* Device bytes a case with these parameters holds (populations, carried
+ * temperature, reduction scratch), for admission against a memory budget. */
+int lbm_case_bytes(const lbm_params *p, uint64_t *bytes);
+
+/* Allocates a case on p->device (replaces the cudaMalloc calls of
+ * src/initial.cu:5-18).  The state is undefined until an init or load call. */
+int lbm_create(const lbm_params *p, lbm_case **out);
+int lbm_destroy(lbm_case *c);
+
+/* init_arrays, src/initial.cu:208-241: rho = 0, u = 0, phi = 0.5. */
+int lbm_init_rest(lbm_case *c, void *stream);
+
+/* Seeded conduction state: T = T_hot - (T_hot-T_cold)*iy/(LY-1) (the profile
+ * of Parallel/initial.cu:89) + amplitude*(2u-1), u uniform in [0,1) from
+ * splitmix64(splitmix64(seed) + idx); zero velocity; f = 0 and g_i = w_i T
+ * (equilibria); carried previous temperature = T. */
+int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stream);
+
+/* Restart state from host FP64 arrays in the reference's file layout
+ * (%09d.dat = rho,ux,uy,uz,phi and fg%09d.dat = f,g; src/initial.cu:110-205).
+ * The engine keeps f, g and the previous-step temperature; the latter is
+ * recovered from uy - sum(c_y f) = g*beta*(phi_prev - t0)/2.  rho, ux, uz
+ * and phi are recomputed from f and g, as the reference's own files hold. */
+int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const double *uy,
+                       const double *uz, const double *phi, const double *f, const double *g);
+
+/* Current state in the same layout: what output_flow and output_fg would
+ * write at this step (src/output.cu:67-146, 379-419).  Any pointer may be
+ * NULL to skip that field. */
+int lbm_store_ref_state(lbm_case *c, double *rho, double *ux, double *uy, double *uz,
+                        double *phi, double *f, double *g);
+
+/* nsteps fused time steps (src/main.cu:27-46), enqueued on `stream`;
+ * asynchronous. */
+int lbm_step(lbm_case *c, int32_t nsteps, void *stream);
+
+/* Device-side reduction of the observables at the current step; waits for
+ * `stream`.  Returns LBM_ERR_DIVERGED (with *out filled) if a NaN/Inf was found. */
+int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream);
+
+/* Vertical profile at the current step, src/output.cu:336-368: for each iy,
+ * out[5*iy + 0..4] = <ux>, <uy>, <uz>, <phi>, phi_rms over the xz plane.
+ * out holds 5*LY doubles; waits for `stream`. */
+int lbm_get_profile(lbm_case *c, double *out, void *stream);
+
+/* Native checkpoint: the device state exactly as held (populations in the
+ * case's storage format and current AA layout, the carried temperature, the
+ * layout flag and the step count), for resuming a case later or evicting it
+ * from HBM.  It has no counterpart in the reference, whose only checkpoint is
+ * the FP64 restart pair above.  lbm_checkpoint_bytes gives the size;
+ * lbm_save_state / lbm_restore_state copy to / from caller memory
+ * (page-locked host memory makes the copies asynchronous) on `stream`;
+ * save returns once the copy is enqueued, so the caller synchronises
+ * `stream` before reading the buffer.  Restore needs a case created with the
+ * same parameters. */
+int lbm_checkpoint_bytes(const lbm_case *c, uint64_t *bytes);
+int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream);
+int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *stream);
+
+/* Parameters and step count of a case. */
+int lbm_get_params(const lbm_case *c, lbm_params *p, lbm_derived *d, int64_t *step);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

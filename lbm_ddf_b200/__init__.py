@@ -1,0 +1,287 @@
+"""B200-native double-distribution lattice Boltzmann engine for 3D
+Rayleigh–Bénard convection — Python host side.
+
+This module mirrors the run surface of Summer536/LBM_DDF's single-GPU path
+(``src/parameters.h`` fields, ``initialize()``, the per-step launches of
+``src/main.cu:27-46`` and the outputs of ``src/output.cu``) over the C ABI of
+``include/lbm_ddf.h``, implemented by the in-tree CUDA library
+``liblbm_ddf.so``.  There is no CPU fallback: importing works without a GPU,
+but every call that touches device state fails with :class:`LbmError` when
+the library or a device is missing.
+
+Axes follow the reference: arrays are indexed ``[z, y, x]`` (x fastest) and
+``y`` is vertical, hot plate below ``iy = 0``, cold plate above ``iy = LY-1``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "liblbm_ddf.so")
+Q = 27
+
+# status codes (include/lbm_ddf.h)
+OK, ERR_ARG, ERR_CUDA, ERR_NOMEM, ERR_DIVERGED, ERR_STATE = 0, -1, -2, -3, -4, -5
+SIDES_WALL, SIDES_PERIODIC = 0, 1
+STORE_F64, STORE_F32, STORE_F16S, STORE_BF16S = 0, 1, 2, 3
+STORAGE_NAMES = {"f64": STORE_F64, "f32": STORE_F32, "f16s": STORE_F16S, "bf16s": STORE_BF16S}
+STORAGE_BYTES = {STORE_F64: 8, STORE_F32: 4, STORE_F16S: 2, STORE_BF16S: 2}
+
+
+class LbmError(RuntimeError):
+    """A C-ABI call returned an error status (the reference would exit())."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+class LbmParams(C.Structure):
+    _fields_ = [
+        ("lx", C.c_int32), ("ly", C.c_int32), ("lz", C.c_int32),
+        ("sides", C.c_int32), ("storage", C.c_int32), ("device", C.c_int32),
+        ("rayleigh", C.c_double), ("prandtl", C.c_double),
+        ("t_hot", C.c_double), ("t_cold", C.c_double),
+        ("gravity", C.c_double), ("beta", C.c_double),
+    ]
+
+
+class LbmDerived(C.Structure):
+    _fields_ = [(k, C.c_double) for k in ("visc", "tau", "u0", "diff", "tauc", "t0")]
+
+
+class LbmObservables(C.Structure):
+    _fields_ = [
+        ("step", C.c_int64),
+        ("nu_bulk", C.c_double), ("nu_top", C.c_double), ("nu_bottom", C.c_double),
+        ("ke", C.c_double), ("re", C.c_double),
+        ("ux_mean", C.c_double), ("uy_mean", C.c_double), ("uz_mean", C.c_double),
+        ("phi_mean", C.c_double),
+        ("diverged", C.c_int32), ("reserved", C.c_int32),
+    ]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+_lib = None
+_dp = C.POINTER(C.c_double)
+
+
+def lib() -> C.CDLL:
+    """The engine library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise LbmError(ERR_STATE, f"CUDA library {LIB_PATH} is not built; run "
+                                      "python -c 'import __graft_entry__ as g; g.build()'")
+        L = C.CDLL(LIB_PATH)
+        vp = C.c_void_p
+        P = C.POINTER(LbmParams)
+        L.lbm_last_error.restype = C.c_char_p
+        L.lbm_abi_version.restype = C.c_int
+        L.lbm_derive.argtypes = [P, C.POINTER(LbmDerived)]
+        L.lbm_case_bytes.argtypes = [P, C.POINTER(C.c_uint64)]
+        L.lbm_create.argtypes = [P, C.POINTER(vp)]
+        L.lbm_destroy.argtypes = [vp]
+        L.lbm_init_rest.argtypes = [vp, vp]
+        L.lbm_init_conduction.argtypes = [vp, C.c_uint64, C.c_double, vp]
+        L.lbm_load_ref_state.argtypes = [vp] + [_dp] * 7
+        L.lbm_store_ref_state.argtypes = [vp] + [_dp] * 7
+        L.lbm_step.argtypes = [vp, C.c_int32, vp]
+        L.lbm_get_observables.argtypes = [vp, C.POINTER(LbmObservables), vp]
+        L.lbm_get_profile.argtypes = [vp, _dp, vp]
+        L.lbm_get_params.argtypes = [vp, P, C.POINTER(LbmDerived), C.POINTER(C.c_int64)]
+        L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
+        L.lbm_save_state.argtypes = [vp, vp, C.c_uint64, vp]
+        L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
+        for name in ("lbm_derive", "lbm_case_bytes", "lbm_create", "lbm_destroy", "lbm_init_rest",
+                     "lbm_init_conduction", "lbm_load_ref_state", "lbm_store_ref_state", "lbm_step",
+                     "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
+                     "lbm_save_state", "lbm_restore_state"):
+            getattr(L, name).restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def check(rc: int) -> int:
+    if rc != OK:
+        raise LbmError(rc, lib().lbm_last_error().decode(errors="replace"))
+    return rc
+
+
+def _stream_handle(stream) -> C.c_void_p:
+    """cudaStream_t from None, an int handle, or an object with .cuda_stream
+    (e.g. torch.cuda.Stream)."""
+    if stream is None:
+        return C.c_void_p(0)
+    if hasattr(stream, "cuda_stream"):
+        return C.c_void_p(int(stream.cuda_stream))
+    return C.c_void_p(int(stream))
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def _buffer(buf):
+    """(address, size in bytes) of a numpy array or a torch tensor."""
+    if hasattr(buf, "data_ptr"):
+        return int(buf.data_ptr()), int(buf.numel() * buf.element_size())
+    a = np.asarray(buf)
+    return int(a.ctypes.data), int(a.nbytes)
+
+
+@dataclass
+class RunSurface:
+    """The fields of the reference's src/parameters.h:5-31, as runtime values,
+    plus the engine's side-wall mode, storage format and device."""
+    LX: int = 400
+    LY: int = 400
+    LZ: int = 400
+    NEND: int = 1000
+    NDIAG: int = 10000
+    NFLOWOUT: int = 10000
+    NNUOUT: int = 10000
+    CONTINUE_STEP: int = 0
+    RAYLEIGH: float = 1.0e7
+    PRANDTL: float = 0.71
+    T_HOT: float = 1.0
+    T_COLD: float = 0.0
+    GRAVITY: float = 1.0
+    BETA: float | None = None     # None: 0.1 / (LY * 5.0) as in src/parameters.h:26
+    sides: int = SIDES_WALL
+    storage: int = STORE_F64
+    device: int = 0
+
+    def params(self) -> LbmParams:
+        beta = self.BETA if self.BETA is not None else 0.1 / (self.LY * 5.0)
+        return LbmParams(lx=self.LX, ly=self.LY, lz=self.LZ, sides=self.sides, storage=self.storage,
+                         device=self.device, rayleigh=self.RAYLEIGH, prandtl=self.PRANDTL,
+                         t_hot=self.T_HOT, t_cold=self.T_COLD, gravity=self.GRAVITY, beta=beta)
+
+
+def make_params(lx, ly, lz, rayleigh=1e5, prandtl=0.71, t_hot=1.0, t_cold=0.0, gravity=1.0,
+                beta=None, sides=SIDES_PERIODIC, storage=STORE_F32, device=0) -> LbmParams:
+    """Parameters with beta chosen for free-fall velocity 0.1 unless given
+    (g*beta*dT*LY = 0.01)."""
+    if isinstance(storage, str):
+        storage = STORAGE_NAMES[storage]
+    if beta is None:
+        beta = 0.01 / (gravity * (t_hot - t_cold) * ly)
+    return LbmParams(lx=lx, ly=ly, lz=lz, sides=sides, storage=storage, device=device,
+                     rayleigh=rayleigh, prandtl=prandtl, t_hot=t_hot, t_cold=t_cold,
+                     gravity=gravity, beta=beta)
+
+
+def derive(p: LbmParams) -> dict:
+    d = LbmDerived()
+    check(lib().lbm_derive(C.byref(p), C.byref(d)))
+    return {k: getattr(d, k) for k, _ in d._fields_}
+
+
+def case_bytes(p: LbmParams) -> int:
+    b = C.c_uint64()
+    check(lib().lbm_case_bytes(C.byref(p), C.byref(b)))
+    return int(b.value)
+
+
+class Case:
+    """One Rayleigh–Bénard case resident in HBM (src/globals.cu's device
+    arrays, owned by this object instead of process globals)."""
+
+    def __init__(self, params: LbmParams):
+        self.params = params
+        h = C.c_void_p()
+        check(lib().lbm_create(C.byref(params), C.byref(h)))
+        self._h = h
+        self.shape = (params.lz, params.ly, params.lx)
+        self.n = params.lx * params.ly * params.lz
+        self.derived = derive(params)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    @property
+    def step_count(self) -> int:
+        s = C.c_int64()
+        check(lib().lbm_get_params(self._h, None, None, C.byref(s)))
+        return int(s.value)
+
+    def init_rest(self, stream=None):
+        check(lib().lbm_init_rest(self._h, _stream_handle(stream)))
+
+    def init_conduction(self, seed: int, amplitude: float = 1e-3, stream=None):
+        check(lib().lbm_init_conduction(self._h, C.c_uint64(seed), amplitude, _stream_handle(stream)))
+
+    def load_ref_state(self, rho, ux, uy, uz, phi, f, g):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, ux, uy, uz, phi, f, g)]
+        check(lib().lbm_load_ref_state(self._h, *[_ptr(a) for a in arrs]))
+
+    def store_ref_state(self, fields=("rho", "ux", "uy", "uz", "phi", "f", "g")) -> dict:
+        out = {}
+        ptrs = []
+        for k in ("rho", "ux", "uy", "uz", "phi", "f", "g"):
+            if k in fields:
+                out[k] = np.empty(((Q,) if k in ("f", "g") else ()) + self.shape, dtype=np.float64)
+                ptrs.append(_ptr(out[k]))
+            else:
+                ptrs.append(None)
+        check(lib().lbm_store_ref_state(self._h, *ptrs))
+        return out
+
+    def step(self, n: int = 1, stream=None):
+        check(lib().lbm_step(self._h, int(n), _stream_handle(stream)))
+
+    def observables(self, stream=None, allow_diverged: bool = False) -> dict:
+        o = LbmObservables()
+        rc = lib().lbm_get_observables(self._h, C.byref(o), _stream_handle(stream))
+        if rc != OK and not (allow_diverged and rc == ERR_DIVERGED):
+            check(rc)
+        return o.as_dict()
+
+    def checkpoint_bytes(self) -> int:
+        b = C.c_uint64()
+        check(lib().lbm_checkpoint_bytes(self._h, C.byref(b)))
+        return int(b.value)
+
+    def save_state(self, buf, stream=None):
+        """Enqueue a copy of the device state into `buf` (anything exposing a
+        writable buffer or a data_ptr(), e.g. a pinned torch uint8 tensor);
+        synchronise `stream` before reading it."""
+        ptr, size = _buffer(buf)
+        check(lib().lbm_save_state(self._h, C.c_void_p(ptr), size, _stream_handle(stream)))
+
+    def restore_state(self, buf, stream=None):
+        ptr, size = _buffer(buf)
+        check(lib().lbm_restore_state(self._h, C.c_void_p(ptr), size, _stream_handle(stream)))
+
+    def profile(self, stream=None) -> np.ndarray:
+        out = np.empty(5 * self.params.ly, dtype=np.float64)
+        check(lib().lbm_get_profile(self._h, _ptr(out), _stream_handle(stream)))
+        return out.reshape(self.params.ly, 5)

@@ -1,0 +1,785 @@
+// engine.cu — single-case engine behind the C ABI of include/lbm_ddf.h.
+//
+// Device state of one case (all in HBM, allocated once at lbm_create):
+//   f, g  : 27 populations each, structure of arrays, population k at
+//           base + k*ps, node idx = (iz*LY + iy)*LX + ix (reference order),
+//           ps = nodes rounded up to 128 elements so that every population
+//           row starts 256-byte aligned;
+//   phip  : previous-step temperature per node (FP64 for F64 storage, else FP32);
+//   scratch: per-block partial sums of the observables reduction and the
+//           reduced result.
+// The layout flag `swapped` records which AA layout the populations are in.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/lbm_ddf.h"
+#include "step.cuh"
+
+using namespace lbm;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int fail(int code, const std::string &msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(call)                                                                         \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess)                                                                 \
+            return fail(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
+    } while (0)
+
+constexpr int kObs = 13;           // partial sums per block, see obs_kernel
+constexpr int kObsThreads = 256;
+constexpr int kStepThreads = 128;
+
+int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
+
+size_t store_bytes(int storage) {
+    switch (storage) {
+    case LBM_STORE_F64: return 8;
+    case LBM_STORE_F32: return 4;
+    case LBM_STORE_F16S:
+    case LBM_STORE_BF16S: return 2;
+    default: return 0;
+    }
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// device kernels besides the step
+// ---------------------------------------------------------------------------
+namespace lbm {
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Per-block partial sums, in FP64, of
+//   0 uy*phi  1 |u|^2  2 ux  3 uy  4 uz  5 phi
+//   6..8  phi on the planes iy = 0, 1, 2
+//   9..11 phi on the planes iy = LY-1, LY-2, LY-3
+//   12 number of nodes with a non-finite moment
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, double *__restrict__ partial) {
+    using R = typename Codec<S>::R;
+    double acc[kObs];
+#pragma unroll
+    for (int k = 0; k < kObs; k++) acc[k] = 0.0;
+    for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < a.nodes; n += gridDim.x * blockDim.x) {
+        const Node g = make_node<PERIODIC>(a, n);
+        R fr[Q], gr[Q];
+        gather<S, SWAPPED>(a, g, fr, gr);
+        const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+        const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
+        acc[0] += uy * phi;
+        acc[1] += ux * ux + uy * uy + uz * uz;
+        acc[2] += ux;
+        acc[3] += uy;
+        acc[4] += uz;
+        acc[5] += phi;
+        if (g.iy == 0) acc[6] += phi;
+        if (g.iy == 1) acc[7] += phi;
+        if (g.iy == 2) acc[8] += phi;
+        if (g.iy == a.ly - 1) acc[9] += phi;
+        if (g.iy == a.ly - 2) acc[10] += phi;
+        if (g.iy == a.ly - 3) acc[11] += phi;
+        if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)m.rho))
+            acc[12] += 1.0;
+    }
+    __shared__ double red[kObs][kObsThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < kObs; k++) {
+        double v = warp_sum(acc[k]);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < kObs) {
+        double s = 0.0;
+        for (int w = 0; w < kObsThreads / 32; w++) s += red[threadIdx.x][w];
+        partial[(size_t)blockIdx.x * kObs + threadIdx.x] = s;
+    }
+}
+
+struct ObsConsts {
+    double nodes, plane, ly, diff, dT, visc;
+    int64_t step;
+};
+
+// Sums the block partials in a fixed order (deterministic) and forms the
+// observables: Nu_bulk of src/output.cu:228-233; Nu_top/bottom of :236-256
+// written with plane sums, <(3T0 - 4T1 + T2)/2> = (3<T0> - 4<T1> + <T2>)/2.
+__global__ void obs_finalize(const double *__restrict__ partial, int nblocks, ObsConsts c,
+                             lbm_observables *__restrict__ out) {
+    __shared__ double tot[kObs];
+    if (threadIdx.x < kObs) {
+        double s = 0.0;
+        for (int b = 0; b < nblocks; b++) s += partial[(size_t)b * kObs + threadIdx.x];
+        tot[threadIdx.x] = s;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const double uyT = tot[0] / c.nodes;
+        out->step = c.step;
+        out->nu_bulk = 1.0 + uyT * c.ly / (c.diff * c.dT);
+        const double b0 = tot[6] / c.plane, b1 = tot[7] / c.plane, b2 = tot[8] / c.plane;
+        const double t0 = tot[9] / c.plane, t1 = tot[10] / c.plane, t2 = tot[11] / c.plane;
+        const double dTdy_bot = (-3.0 * b0 + 4.0 * b1 - b2) / 2.0;
+        const double dTdy_top = (3.0 * t0 - 4.0 * t1 + t2) / 2.0;
+        out->nu_top = -dTdy_top * c.ly / c.dT;
+        out->nu_bottom = -dTdy_bot * c.ly / c.dT;
+        const double usq = tot[1] / c.nodes;
+        out->ke = 0.5 * usq;
+        out->re = sqrt(usq) * c.ly / c.visc;
+        out->ux_mean = tot[2] / c.nodes;
+        out->uy_mean = tot[3] / c.nodes;
+        out->uz_mean = tot[4] / c.nodes;
+        out->phi_mean = tot[5] / c.nodes;
+        out->diverged = tot[12] > 0.0 ? 1 : 0;
+        out->reserved = 0;
+    }
+}
+
+// Vertical profile, src/output.cu:336-368: one block per xz plane iy.
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void __launch_bounds__(kObsThreads) profile_kernel(const StepArgs<S> a, double *__restrict__ out) {
+    using R = typename Codec<S>::R;
+    const int iy = blockIdx.x;
+    double acc[5] = {0, 0, 0, 0, 0};
+    const uint32_t cnt = (uint32_t)a.lx * (uint32_t)a.lz;
+    for (uint32_t t = threadIdx.x; t < cnt; t += blockDim.x) {
+        const uint32_t iz = t / (uint32_t)a.lx, ix = t - iz * (uint32_t)a.lx;
+        const uint32_t n = (iz * (uint32_t)a.ly + (uint32_t)iy) * (uint32_t)a.lx + ix;
+        const Node g = make_node<PERIODIC>(a, n);
+        R fr[Q], gr[Q];
+        gather<S, SWAPPED>(a, g, fr, gr);
+        const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+        acc[0] += (double)m.ux;
+        acc[1] += (double)m.uy;
+        acc[2] += (double)m.uz;
+        acc[3] += (double)m.phi;
+        acc[4] += (double)m.phi * (double)m.phi;
+    }
+    __shared__ double red[5][kObsThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        double v = warp_sum(acc[k]);
+        if (lane == 0) red[k][warp] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double s[5];
+        for (int k = 0; k < 5; k++) {
+            s[k] = 0.0;
+            for (int w = 0; w < (int)(blockDim.x / 32); w++) s[k] += red[k][w];
+        }
+        const double c = (double)cnt;
+        const double ap = s[3] / c;
+        out[5 * iy + 0] = s[0] / c;
+        out[5 * iy + 1] = s[1] / c;
+        out[5 * iy + 2] = s[2] / c;
+        out[5 * iy + 3] = ap;
+        out[5 * iy + 4] = sqrt(s[4] / c - ap * ap);
+    }
+}
+
+// One population (which 0 = f, 1 = g; index k), decoded, natural order.
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void export_pop_kernel(const StepArgs<S> a, int which, int k, double *__restrict__ out) {
+    using C = Codec<S>;
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    const Node g = make_node<PERIODIC>(a, n);
+    const S *base = which ? a.g : a.f;
+    double v = 0.0;
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        if (K == k) {
+            const S s = load_pop<S, SWAPPED, K>(base, a.ps, g);
+            v = which ? (double)C::template g_in<K>(s, a.t0) : (double)C::template f_in<K>(s, a.t0);
+        }
+    });
+    out[n] = v;
+}
+
+// rho, ux, uy, uz, phi as the reference's macrovar leaves them (src/macrovar.cu:3-34).
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void export_macro_kernel(const StepArgs<S> a, double *__restrict__ out /* 5 x nodes */) {
+    using R = typename Codec<S>::R;
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    const Node g = make_node<PERIODIC>(a, n);
+    R fr[Q], gr[Q];
+    gather<S, SWAPPED>(a, g, fr, gr);
+    const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+    const size_t N = a.nodes;
+    out[n] = (double)m.rho;
+    out[N + n] = (double)m.ux;
+    out[2 * N + n] = (double)m.uy;
+    out[3 * N + n] = (double)m.uz;
+    out[4 * N + n] = (double)m.phi;
+}
+
+// Writes one population in the natural layout from FP64 values.
+template <class S>
+__global__ void import_pop_kernel(const StepArgs<S> a, int which, int k, const double *__restrict__ in) {
+    using C = Codec<S>;
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    S *base = which ? a.g : a.f;
+    const double v = in[n];
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        if (K == k) {
+            using R = typename C::R;
+            base[(int64_t)K * a.ps + n] = which ? C::template g_out<K>((R)v, a.t0) : C::template f_out<K>((R)v, a.t0);
+        }
+    });
+}
+
+template <class S>
+__global__ void import_phip_kernel(const StepArgs<S> a, const double *__restrict__ in) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    a.phip[n] = (typename Codec<S>::P)in[n];
+}
+
+__device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+// Conduction (mode 1) or rest (mode 0, src/initial.cu:208-241) state.
+// Temperatures are formed in FP64 with explicit round-to-nearest operations,
+// in the order T = T_hot - ((T_hot - T_cold) * iy) / (LY - 1.0), then
+// T + amplitude*(2u - 1), so every build gives the same bits.
+template <class S>
+__global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, double amplitude, double t_hot,
+                            double t_cold) {
+    using C = Codec<S>;
+    using R = typename C::R;
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    double t = 0.5;
+    if (mode == 1) {
+        const uint32_t q = a.div_lx.div(n);
+        const uint32_t z = a.div_ly.div(q);
+        const int iy = (int)(q - z * (uint32_t)a.ly);
+        const uint64_t r = splitmix64(seed_key + (uint64_t)n);
+        const double u = (double)(r >> 11) * (1.0 / 9007199254740992.0);
+        t = __dsub_rn(t_hot, __ddiv_rn(__dmul_rn(__dsub_rn(t_hot, t_cold), (double)iy), __dsub_rn((double)a.ly, 1.0)));
+        t = __dadd_rn(t, __dmul_rn(amplitude, __dsub_rn(__dmul_rn(2.0, u), 1.0)));
+    }
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        const double gk = __dmul_rn(wd(K), t);
+        a.f[(int64_t)K * a.ps + n] = C::template f_out<K>((R)0, a.t0);
+        a.g[(int64_t)K * a.ps + n] = C::template g_out<K>((R)gk, a.t0);
+    });
+    a.phip[n] = (typename C::P)t;
+}
+
+}  // namespace lbm
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+struct lbm_case {
+    lbm_params p;
+    lbm_derived d;
+    int64_t nodes = 0, ps = 0;
+    int64_t step = 0;
+    bool swapped = false;
+    bool initialised = false;
+    void *f = nullptr, *g = nullptr, *phip = nullptr;
+    double *partial = nullptr;           // obs partial sums
+    lbm_observables *d_obs = nullptr;    // reduced observables (device)
+    int obs_blocks = 0;
+};
+
+namespace {
+
+int check_params(const lbm_params *p) {
+    if (!p) return fail(LBM_ERR_ARG, "params is NULL");
+    if (p->lx < 2 || p->ly < 3 || p->lz < 2)
+        return fail(LBM_ERR_ARG, "grid must be at least 2 x 3 x 2 (LY >= 3 for the plate gradients)");
+    const double nodes = (double)p->lx * (double)p->ly * (double)p->lz;
+    if (nodes > 2147483647.0) return fail(LBM_ERR_ARG, "more than 2^31-1 nodes in one case");
+    if (p->sides != LBM_SIDES_WALL && p->sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "bad sides");
+    if (store_bytes(p->storage) == 0) return fail(LBM_ERR_ARG, "bad storage");
+    if (!(p->rayleigh > 0) || !(p->prandtl > 0)) return fail(LBM_ERR_ARG, "Ra and Pr must be positive");
+    if (!(p->t_hot > p->t_cold)) return fail(LBM_ERR_ARG, "T_hot must exceed T_cold");
+    if (!(p->gravity * p->beta > 0)) return fail(LBM_ERR_ARG, "gravity*beta must be positive");
+    return LBM_OK;
+}
+
+void derive(const lbm_params *p, lbm_derived *d) {
+    const double ly = (double)p->ly;
+    d->visc = ly * std::sqrt(p->gravity * p->beta * (p->t_hot - p->t_cold) * ly * p->prandtl / p->rayleigh);
+    d->tau = 3.0 * d->visc + 0.5;
+    d->u0 = std::sqrt(p->gravity * p->beta * (p->t_hot - p->t_cold) * ly);
+    d->diff = d->visc / p->prandtl;
+    d->tauc = 3.0 * d->diff + 0.5;
+    d->t0 = 0.5 * (p->t_cold + p->t_hot);
+}
+
+int obs_blocks_for(int64_t nodes) {
+    int64_t b = (nodes + kObsThreads - 1) / kObsThreads;
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
+}
+
+template <class S> StepArgs<S> make_args(const lbm_case *c) {
+    using R = typename Codec<S>::R;
+    StepArgs<S> a;
+    a.f = (S *)c->f;
+    a.g = (S *)c->g;
+    a.f_st = (S *)c->f;
+    a.g_st = (S *)c->g;
+    a.phip = (typename Codec<S>::P *)c->phip;
+    a.ps = c->ps;
+    a.lx = c->p.lx;
+    a.ly = c->p.ly;
+    a.lz = c->p.lz;
+    a.nodes = (uint32_t)c->nodes;
+    a.div_lx = FastDiv((uint32_t)c->p.lx);
+    a.div_ly = FastDiv((uint32_t)c->p.ly);
+    a.omega_f = (R)(1.0 / c->d.tau);
+    a.omega_g = (R)(1.0 / c->d.tauc);
+    a.force_fac = (R)(1.0 - 0.5 / c->d.tau);
+    a.gb = (R)(c->p.gravity * c->p.beta);
+    a.t0 = (R)c->d.t0;
+    a.t_hot = (R)c->p.t_hot;
+    a.t_cold = (R)c->p.t_cold;
+    return a;
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+inline unsigned grid_for(int64_t nodes, int threads) { return (unsigned)((nodes + threads - 1) / threads); }
+
+// Calls fn(tag<S>) for the case's storage type.
+template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
+    switch (c->p.storage) {
+    case LBM_STORE_F64: return fn((double *)nullptr);
+    case LBM_STORE_F32: return fn((float *)nullptr);
+    case LBM_STORE_F16S: return fn((__half *)nullptr);
+    case LBM_STORE_BF16S: return fn((__nv_bfloat16 *)nullptr);
+    }
+    return fail(LBM_ERR_ARG, "bad storage");
+}
+
+template <class S, bool SW, bool PER> void launch_step_t(const StepArgs<S> &a, int64_t nodes, cudaStream_t st) {
+    step_kernel<S, SW, PER><<<grid_for(nodes, kStepThreads), kStepThreads, 0, st>>>(a);
+}
+
+template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    const bool per = c->p.sides == LBM_SIDES_PERIODIC;
+    if (c->swapped) {
+        if (per) launch_step_t<S, true, true>(a, c->nodes, st);
+        else launch_step_t<S, true, false>(a, c->nodes, st);
+    } else {
+        if (per) launch_step_t<S, false, true>(a, c->nodes, st);
+        else launch_step_t<S, false, false>(a, c->nodes, st);
+    }
+}
+
+// Dispatch a (SWAPPED, PERIODIC)-templated launch for the case's current layout.
+#define LBM_DISPATCH_LAYOUT(c, KERNEL, GRID, BLOCK, STREAM, ...)                         \
+    do {                                                                                  \
+        const bool per_ = (c)->p.sides == LBM_SIDES_PERIODIC;                             \
+        if ((c)->swapped) {                                                               \
+            if (per_) KERNEL<S, true, true><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);      \
+            else KERNEL<S, true, false><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);          \
+        } else {                                                                          \
+            if (per_) KERNEL<S, false, true><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);     \
+            else KERNEL<S, false, false><<<GRID, BLOCK, 0, STREAM>>>(__VA_ARGS__);         \
+        }                                                                                 \
+    } while (0)
+
+int check_case(const lbm_case *c, bool need_state) {
+    if (!c) return fail(LBM_ERR_ARG, "case is NULL");
+    if (need_state && !c->initialised) return fail(LBM_ERR_STATE, "case has no state yet (init or load first)");
+    return LBM_OK;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// C ABI
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char *lbm_last_error(void) { return g_last_error.c_str(); }
+int lbm_abi_version(void) { return LBM_DDF_ABI_VERSION; }
+
+int lbm_derive(const lbm_params *p, lbm_derived *out) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    derive(p, out);
+    return LBM_OK;
+}
+
+int lbm_case_bytes(const lbm_params *p, uint64_t *bytes) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!bytes) return fail(LBM_ERR_ARG, "bytes is NULL");
+    const int64_t nodes = (int64_t)p->lx * p->ly * p->lz;
+    const int64_t ps = round_up(nodes, 128);
+    const uint64_t pop = 2ull * Q * (uint64_t)ps * store_bytes(p->storage);
+    const uint64_t carry = (uint64_t)round_up(nodes, 128) * (p->storage == LBM_STORE_F64 ? 8 : 4);
+    const uint64_t scratch = (uint64_t)obs_blocks_for(nodes) * kObs * 8 + 256;
+    *bytes = pop + carry + scratch;
+    return LBM_OK;
+}
+
+int lbm_create(const lbm_params *p, lbm_case **out) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    lbm_case *c = new (std::nothrow) lbm_case();
+    if (!c) return fail(LBM_ERR_NOMEM, "host allocation failed");
+    c->p = *p;
+    derive(p, &c->d);
+    c->nodes = (int64_t)p->lx * p->ly * p->lz;
+    c->ps = round_up(c->nodes, 128);
+    c->obs_blocks = obs_blocks_for(c->nodes);
+    DeviceGuard dg(p->device);
+    const size_t sb = store_bytes(p->storage);
+    const size_t pop_bytes = (size_t)Q * (size_t)c->ps * sb;
+    const size_t carry_bytes = (size_t)c->ps * (p->storage == LBM_STORE_F64 ? 8 : 4);
+    cudaError_t e = cudaMalloc(&c->f, pop_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->g, pop_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->phip, carry_bytes);
+    if (e == cudaSuccess) e = cudaMalloc(&c->partial, (size_t)c->obs_blocks * kObs * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_obs, sizeof(lbm_observables));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        lbm_destroy(c);
+        return fail(e == cudaErrorMemoryAllocation ? LBM_ERR_NOMEM : LBM_ERR_CUDA,
+                    std::string("device allocation failed: ") + cudaGetErrorString(e));
+    }
+    *out = c;
+    return LBM_OK;
+}
+
+int lbm_destroy(lbm_case *c) {
+    if (!c) return LBM_OK;
+    DeviceGuard dg(c->p.device);
+    cudaFree(c->f);
+    cudaFree(c->g);
+    cudaFree(c->phip);
+    cudaFree(c->partial);
+    cudaFree(c->d_obs);
+    delete c;
+    return LBM_OK;
+}
+
+static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, void *stream) {
+    int rc = check_case(c, false);
+    if (rc) return rc;
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const uint64_t key = [&] {
+        uint64_t x = seed + 0x9E3779B97F4A7C15ull;
+        x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+        x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+        return x ^ (x >> 31);
+    }();
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        init_kernel<S><<<grid_for(c->nodes, 256), 256, 0, st>>>(a, mode, key, amplitude, c->p.t_hot, c->p.t_cold);
+        return LBM_OK;
+    });
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
+    c->swapped = false;
+    c->step = 0;
+    c->initialised = true;
+    return LBM_OK;
+}
+
+int lbm_init_rest(lbm_case *c, void *stream) { return init_common(c, 0, 0, 0.0, stream); }
+
+int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stream) {
+    return init_common(c, 1, seed, amplitude, stream);
+}
+
+int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const double *uy, const double *uz,
+                       const double *phi, const double *f, const double *g) {
+    (void)rho; (void)ux; (void)uz; (void)phi;
+    int rc = check_case(c, false);
+    if (rc) return rc;
+    if (!uy || !f || !g) return fail(LBM_ERR_ARG, "uy, f and g are required");
+    DeviceGuard dg(c->p.device);
+    const int64_t N = c->nodes;
+    // previous-step temperature from uy = sum(c_y f) + g*beta*(phi_prev - t0)/2
+    std::vector<double> pp((size_t)N);
+    const double gb = c->p.gravity * c->p.beta;
+    for (int64_t i = 0; i < N; i++) {
+        double jy = 0.0;
+        for (int k = 0; k < Q; k++) {
+            if (cy(k) > 0) jy += f[(size_t)k * N + i];
+            if (cy(k) < 0) jy -= f[(size_t)k * N + i];
+        }
+        pp[(size_t)i] = c->d.t0 + 2.0 * (uy[i] - jy) / gb;
+    }
+    double *stage = nullptr;
+    CUDA_TRY(cudaMalloc(&stage, (size_t)N * sizeof(double)));
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        for (int which = 0; which < 2; which++)
+            for (int k = 0; k < Q; k++) {
+                const double *src = (which ? g : f) + (size_t)k * N;
+                cudaError_t e = cudaMemcpy(stage, src, (size_t)N * sizeof(double), cudaMemcpyHostToDevice);
+                if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+                import_pop_kernel<S><<<grid_for(N, 256), 256>>>(a, which, k, stage);
+            }
+        cudaError_t e = cudaMemcpy(stage, pp.data(), (size_t)N * sizeof(double), cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+        import_phip_kernel<S><<<grid_for(N, 256), 256>>>(a, stage);
+        return LBM_OK;
+    });
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaFree(stage);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    c->swapped = false;
+    c->step = 0;
+    c->initialised = true;
+    return LBM_OK;
+}
+
+int lbm_store_ref_state(lbm_case *c, double *rho, double *ux, double *uy, double *uz, double *phi, double *f,
+                        double *g) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    DeviceGuard dg(c->p.device);
+    const int64_t N = c->nodes;
+    CUDA_TRY(cudaDeviceSynchronize());
+    double *stage = nullptr;
+    CUDA_TRY(cudaMalloc(&stage, (size_t)N * 5 * sizeof(double)));
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        if (rho || ux || uy || uz || phi) {
+            LBM_DISPATCH_LAYOUT(c, export_macro_kernel, grid_for(N, 256), 256, (cudaStream_t)0, a, stage);
+            double *dst[5] = {rho, ux, uy, uz, phi};
+            for (int k = 0; k < 5; k++)
+                if (dst[k]) {
+                    cudaError_t e = cudaMemcpy(dst[k], stage + (size_t)k * N, (size_t)N * sizeof(double),
+                                               cudaMemcpyDeviceToHost);
+                    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+                }
+        }
+        for (int which = 0; which < 2; which++) {
+            double *dst = which ? g : f;
+            if (!dst) continue;
+            for (int k = 0; k < Q; k++) {
+                LBM_DISPATCH_LAYOUT(c, export_pop_kernel, grid_for(N, 256), 256, (cudaStream_t)0, a, which, k,
+                                    stage);
+                cudaError_t e = cudaMemcpy(dst + (size_t)k * N, stage, (size_t)N * sizeof(double),
+                                           cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+            }
+        }
+        return LBM_OK;
+    });
+    cudaError_t e = cudaGetLastError();
+    cudaFree(stage);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    return LBM_OK;
+}
+
+int lbm_step(lbm_case *c, int32_t nsteps, void *stream) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(LBM_ERR_ARG, "nsteps < 0");
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        for (int s = 0; s < nsteps; s++) {
+            launch_step<S>(c, a, st);
+            c->swapped = !c->swapped;
+        }
+        return LBM_OK;
+    });
+    if (rc) return rc;
+    c->step += nsteps;
+    CUDA_TRY(cudaGetLastError());
+    return LBM_OK;
+}
+
+int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
+        ObsConsts k;
+        k.nodes = (double)c->nodes;
+        k.plane = (double)c->p.lx * (double)c->p.lz;
+        k.ly = (double)c->p.ly;
+        k.diff = c->d.diff;
+        k.dT = c->p.t_hot - c->p.t_cold;
+        k.visc = c->d.visc;
+        k.step = c->step;
+        obs_finalize<<<1, 32, 0, st>>>(c->partial, c->obs_blocks, k, c->d_obs);
+        return LBM_OK;
+    });
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, c->d_obs, sizeof(lbm_observables), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    if (out->diverged) return fail(LBM_ERR_DIVERGED, "NaN/Inf in the macroscopic fields");
+    return LBM_OK;
+}
+
+int lbm_get_profile(lbm_case *c, double *out, void *stream) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    double *dprof = nullptr;
+    CUDA_TRY(cudaMalloc(&dprof, (size_t)5 * c->p.ly * sizeof(double)));
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(c);
+        LBM_DISPATCH_LAYOUT(c, profile_kernel, c->p.ly, kObsThreads, st, a, dprof);
+        return LBM_OK;
+    });
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(out, dprof, (size_t)5 * c->p.ly * sizeof(double), cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    cudaFree(dprof);
+    if (rc) return rc;
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    return LBM_OK;
+}
+
+// Checkpoint image: header, f, g, phip (each region 256-byte aligned).
+struct CheckpointHeader {
+    char magic[8];          // "LBMDDF1\0"
+    lbm_params p;
+    int64_t step;
+    int32_t swapped;
+    int32_t reserved;
+    int64_t ps;
+};
+
+static uint64_t ckpt_layout(const lbm_case *c, uint64_t *off_f, uint64_t *off_g, uint64_t *off_p,
+                            uint64_t *pop_bytes, uint64_t *carry_bytes) {
+    const uint64_t hb = (uint64_t)round_up(sizeof(CheckpointHeader), 256);
+    *pop_bytes = (uint64_t)Q * (uint64_t)c->ps * store_bytes(c->p.storage);
+    *carry_bytes = (uint64_t)c->ps * (c->p.storage == LBM_STORE_F64 ? 8 : 4);
+    *off_f = hb;
+    *off_g = hb + *pop_bytes;
+    *off_p = hb + 2 * *pop_bytes;
+    return *off_p + *carry_bytes;
+}
+
+int lbm_checkpoint_bytes(const lbm_case *c, uint64_t *bytes) {
+    if (!c || !bytes) return fail(LBM_ERR_ARG, "NULL argument");
+    uint64_t a, b, d, e, f;
+    *bytes = ckpt_layout(c, &a, &b, &d, &e, &f);
+    return LBM_OK;
+}
+
+int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    uint64_t of, og, op, pb, cb;
+    const uint64_t need = ckpt_layout(c, &of, &og, &op, &pb, &cb);
+    if (!host || bytes < need) return fail(LBM_ERR_ARG, "checkpoint buffer missing or too small");
+    DeviceGuard dg(c->p.device);
+    CheckpointHeader h;
+    std::memset(&h, 0, sizeof h);
+    std::memcpy(h.magic, "LBMDDF1", 8);
+    h.p = c->p;
+    h.step = c->step;
+    h.swapped = c->swapped ? 1 : 0;
+    h.ps = c->ps;
+    std::memcpy(host, &h, sizeof h);
+    cudaStream_t st = (cudaStream_t)stream;
+    char *b = (char *)host;
+    CUDA_TRY(cudaMemcpyAsync(b + of, c->f, pb, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(b + og, c->g, pb, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(b + op, c->phip, cb, cudaMemcpyDeviceToHost, st));
+    return LBM_OK;
+}
+
+int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *stream) {
+    int rc = check_case(c, false);
+    if (rc) return rc;
+    uint64_t of, og, op, pb, cb;
+    const uint64_t need = ckpt_layout(c, &of, &og, &op, &pb, &cb);
+    if (!host || bytes < need) return fail(LBM_ERR_ARG, "checkpoint buffer missing or too small");
+    CheckpointHeader h;
+    std::memcpy(&h, host, sizeof h);
+    if (std::memcmp(h.magic, "LBMDDF1", 8) != 0) return fail(LBM_ERR_ARG, "not an engine checkpoint");
+    if (h.p.lx != c->p.lx || h.p.ly != c->p.ly || h.p.lz != c->p.lz || h.p.storage != c->p.storage ||
+        h.p.sides != c->p.sides || h.ps != c->ps || h.p.rayleigh != c->p.rayleigh || h.p.prandtl != c->p.prandtl ||
+        h.p.beta != c->p.beta || h.p.gravity != c->p.gravity || h.p.t_hot != c->p.t_hot || h.p.t_cold != c->p.t_cold)
+        return fail(LBM_ERR_ARG, "checkpoint was taken from a case with other parameters");
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const char *b = (const char *)host;
+    CUDA_TRY(cudaMemcpyAsync(c->f, b + of, pb, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->g, b + og, pb, cudaMemcpyHostToDevice, st));
+    CUDA_TRY(cudaMemcpyAsync(c->phip, b + op, cb, cudaMemcpyHostToDevice, st));
+    c->step = h.step;
+    c->swapped = h.swapped != 0;
+    c->initialised = true;
+    return LBM_OK;
+}
+
+int lbm_get_params(const lbm_case *c, lbm_params *p, lbm_derived *d, int64_t *step) {
+    if (!c) return fail(LBM_ERR_ARG, "case is NULL");
+    if (p) *p = c->p;
+    if (d) *d = c->d;
+    if (step) *step = c->step;
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,248 @@
+// step.cuh — the fused LBM-DDF time step: moments, BGK collision of f with the
+// Boussinesq force, BGK collision of g, and streaming with halfway bounce-back
+// and anti-bounce-back plates, for one node per thread, in place (AA pattern).
+//
+// What one step computes is the reference's six-launch step
+// (Summer536/LBM_DDF src/main.cu:27-46):
+//   forcing     F_y = g*beta*(phi^{n-1} - t0)                    src/macrovar.cu:36-47
+//   collide f   BGK to feq(rho, u) + (1 - 1/(2 tau)) F_y 3(c_y - u_y) feq(1, u)
+//                                                               src/collision.cu:3-33
+//   collide g   BGK to geq = w phi (1 + 3c.u + 4.5(c.u)^2 - 1.5u^2)  src/collision.cu:52-64
+//   stream f/g  with the wall rules of src/streaming.cu:59-124, 183-250
+//   macrovar    rho = sum f, u = sum c f + F/2, phi = sum g      src/macrovar.cu:3-34
+// fused into a single pass.  The moments of step n are recomputed from the
+// populations at the start of step n+1; the only extra per-node state is the
+// previous-step temperature phi^{n-1} ("phip"), because the stored velocity of
+// the reference carries the force of the previous step (u^n = sum c f^n +
+// g*beta*(phi^{n-1} - t0)/2) and the anti-bounce-back uses rho^{n-1}.
+//
+// AA pattern (Bailey et al., ICPP 2009).  One array per distribution holds
+// the populations in one of two layouts:
+//   natural : slot k of node x holds f_k(x) after streaming;
+//   swapped : slot k of node x holds the post-collision f*_{opp k}(x), not
+//             yet streamed.
+// From natural, a step reads slot k of x and writes f*_i to slot opp(i) of x
+// (all accesses local).  From swapped, a step reads population k of x from
+// slot opp(k) of x - c_k, and writes f*_i to slot i of x + c_i (the set of
+// locations a node reads is the set it writes, so no two threads touch the
+// same word).  Walls: a population that would leave the box through a wall
+// is kept at the node, in the slot its reflection is read from next step,
+// with the anti-bounce-back transform applied when it is written; the
+// rho^{n-1} this needs is the pre-collision density of the same node.
+//
+// Wall precedence (reference "last write wins", src/streaming.cu:59-124,
+// 183-250, faces applied x-, x+, y-, y+, z-, z+): for g a population that
+// crosses a z face is bounced back plainly even if it also crosses a y face;
+// otherwise crossing a y face gives anti-bounce-back.  For f every rule is the
+// same plain bounce-back.
+#pragma once
+
+#include "lattice.cuh"
+
+namespace lbm {
+
+template <class S> struct StepArgs {
+    using R = typename Codec<S>::R;
+    using P = typename Codec<S>::P;
+    S *f;              // 27 populations, population k at f + k*ps
+    S *g;
+    // The same two arrays again, used only for the stores.  In the
+    // natural-layout step every store address equals a load address; forming
+    // it from a separate base keeps the compiler from holding all 54 load
+    // addresses live across the collision (which costs ~110 registers).
+    S *f_st;
+    S *g_st;
+    P *phip;           // previous-step temperature, one per node
+    int64_t ps;        // population stride in elements (>= nodes)
+    int32_t lx, ly, lz;
+    uint32_t nodes;
+    FastDiv div_lx, div_ly;
+    R omega_f;         // 1/tau
+    R omega_g;         // 1/tauc
+    R force_fac;       // 1 - 1/(2 tau)
+    R gb;              // gravity*beta
+    R t0, t_hot, t_cold;
+};
+
+// Geometry of one node: coordinates, and node-index displacements to the
+// neighbours along each axis (periodic wrap folded in), with validity flags.
+struct Node {
+    uint32_t n;
+    int32_t ix, iy, iz;
+    int32_t dxm, dxp, dym, dyp, dzm, dzp;
+    bool vxm, vxp, vym, vyp, vzm, vzp;
+};
+
+template <bool PERIODIC, class A>
+__device__ __forceinline__ Node make_node(const A &a, uint32_t n) {
+    Node g;
+    g.n = n;
+    uint32_t q = a.div_lx.div(n);
+    g.ix = (int32_t)(n - q * (uint32_t)a.lx);
+    uint32_t z = a.div_ly.div(q);
+    g.iy = (int32_t)(q - z * (uint32_t)a.ly);
+    g.iz = (int32_t)z;
+    const int32_t plane = a.lx * a.ly;
+    g.dym = -a.lx;
+    g.dyp = a.lx;
+    g.vym = g.iy > 0;
+    g.vyp = g.iy < a.ly - 1;
+    if (PERIODIC) {
+        g.dxm = g.ix > 0 ? -1 : a.lx - 1;
+        g.dxp = g.ix < a.lx - 1 ? 1 : 1 - a.lx;
+        g.dzm = g.iz > 0 ? -plane : (a.lz - 1) * plane;
+        g.dzp = g.iz < a.lz - 1 ? plane : (1 - a.lz) * plane;
+        g.vxm = g.vxp = g.vzm = g.vzp = true;
+    } else {
+        g.dxm = -1;
+        g.dxp = 1;
+        g.dzm = -plane;
+        g.dzp = plane;
+        g.vxm = g.ix > 0;
+        g.vxp = g.ix < a.lx - 1;
+        g.vzm = g.iz > 0;
+        g.vzp = g.iz < a.lz - 1;
+    }
+    return g;
+}
+
+// displacement (in nodes) and validity of the neighbour x + (DX, DY, DZ)
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ int32_t disp(const Node &g) {
+    return (DX < 0 ? g.dxm : DX > 0 ? g.dxp : 0) + (DY < 0 ? g.dym : DY > 0 ? g.dyp : 0) +
+           (DZ < 0 ? g.dzm : DZ > 0 ? g.dzp : 0);
+}
+template <int DX, int DY, int DZ>
+__device__ __forceinline__ bool inside(const Node &g) {
+    return (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) && (DY < 0 ? g.vym : DY > 0 ? g.vyp : true) &&
+           (DZ < 0 ? g.vzm : DZ > 0 ? g.vzp : true);
+}
+
+// Population k of node g at the current time, from either layout.
+template <class S, bool SWAPPED, int K>
+__device__ __forceinline__ S load_pop(const S *__restrict__ base, int64_t ps, const Node &g) {
+    if (!SWAPPED) return base[(int64_t)K * ps + g.n];
+    constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
+    if (inside<DX, DY, DZ>(g)) return base[(int64_t)opp(K) * ps + (int64_t)((int64_t)g.n + disp<DX, DY, DZ>(g))];
+    return base[(int64_t)K * ps + g.n];
+}
+
+template <class S, bool SWAPPED>
+__device__ __forceinline__ void gather(const StepArgs<S> &a, const Node &g, typename Codec<S>::R (&fr)[Q],
+                                       typename Codec<S>::R (&gr)[Q]) {
+    using C = Codec<S>;
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K>(a.f, a.ps, g), a.t0);
+        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K>(a.g, a.ps, g), a.t0);
+    });
+}
+
+// Moments of the populations at one node.  u carries the previous step's
+// half force, as the reference's stored velocity does (src/macrovar.cu:28-30).
+template <class R> struct Moments {
+    R rho, ux, uy, uz, phi;
+};
+
+template <class R>
+__device__ __forceinline__ Moments<R> moments(const R (&fr)[Q], const R (&gr)[Q], R phip, R gb, R t0) {
+    Moments<R> m;
+    R rho = 0, jx = 0, jy = 0, jz = 0, phi = 0;
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        rho += fr[K];
+        if (cx(K) > 0) jx += fr[K];
+        if (cx(K) < 0) jx -= fr[K];
+        if (cy(K) > 0) jy += fr[K];
+        if (cy(K) < 0) jy -= fr[K];
+        if (cz(K) > 0) jz += fr[K];
+        if (cz(K) < 0) jz -= fr[K];
+        phi += gr[K];
+    });
+    m.rho = rho;
+    m.ux = jx;
+    m.uy = jy + R(0.5) * (gb * (phip - t0));
+    m.uz = jz;
+    m.phi = phi;
+    return m;
+}
+
+// BGK collision of f (with the buoyancy force) and g, in place on fr/gr.
+template <class R>
+__device__ __forceinline__ void collide(R (&fr)[Q], R (&gr)[Q], const Moments<R> &m, R omega_f, R omega_g,
+                                        R force_fac, R gb, R t0) {
+    const R uv = R(3) * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+    const R fy = gb * (m.phi - t0);           // force of this step, from phi^{n-1}
+    const R kf = R(3) * force_fac * fy;
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        constexpr R w = R(wd(K));
+        R cu = R(0);
+        if (cx(K) > 0) cu += m.ux;
+        if (cx(K) < 0) cu -= m.ux;
+        if (cy(K) > 0) cu += m.uy;
+        if (cy(K) < 0) cu -= m.uy;
+        if (cz(K) > 0) cu += m.uz;
+        if (cz(K) < 0) cu -= m.uz;
+        const R eu = R(3) * cu;
+        const R p = eu + R(0.5) * (eu * eu - uv);   // velocity part of the equilibria
+        const R feq = w * (m.rho + p);
+        const R feq0 = w * (R(1) + p);
+        const R fo = fr[K];
+        fr[K] = fo - omega_f * (fo - feq) + kf * (R(cy(K)) - m.uy) * feq0;
+        const R go = gr[K];
+        gr[K] = go - omega_g * (go - m.phi * feq0);
+    });
+}
+
+// Write the post-collision populations of node g to where the next step
+// reads them.  rho is the node's pre-collision density (for anti-bounce-back).
+template <class S, bool SWAPPED, bool PERIODIC>
+__device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, const typename Codec<S>::R (&fr)[Q],
+                                        const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
+    using C = Codec<S>;
+    using R = typename C::R;
+    const R abb_hot = R(2) * a.t_hot * (R(1) + rho);
+    const R abb_cold = R(2) * a.t_cold * (R(1) + rho);
+    Unroll<0, Q>::run([&](auto ii) {
+        constexpr int I = decltype(ii)::value;
+        constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
+        R fv = fr[I];
+        R gv = gr[I];
+        const bool out_y = (DY < 0 && !g.vym) || (DY > 0 && !g.vyp);
+        const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        if (DY != 0 && out_y && !out_z) gv = -gv + R(wd(I)) * (DY < 0 ? abb_hot : abb_cold);
+        int64_t off;
+        if (!SWAPPED) {
+            off = (int64_t)opp(I) * a.ps + g.n;
+        } else if (inside<DX, DY, DZ>(g)) {
+            off = (int64_t)I * a.ps + (int64_t)((int64_t)g.n + disp<DX, DY, DZ>(g));
+        } else {
+            off = (int64_t)opp(I) * a.ps + g.n;
+        }
+        a.f_st[off] = C::template f_out<I>(fv, a.t0);
+        a.g_st[off] = C::template g_out<I>(gv, a.t0);
+    });
+}
+
+// Resident blocks per SM the register allocation is sized for: 3 x 128
+// threads (<= 168 registers) for 4-byte and 2-byte storage, 2 (<= 255) for
+// FP64, which holds 54 doubles across the collision.
+template <class S> struct StepOccupancy { static constexpr int value = sizeof(S) == 8 ? 2 : 3; };
+
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
+    using R = typename Codec<S>::R;
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    const Node g = make_node<PERIODIC>(a, n);
+    R fr[Q], gr[Q];
+    gather<S, SWAPPED>(a, g, fr, gr);
+    const R pp = (R)a.phip[n];
+    const Moments<R> m = moments(fr, gr, pp, a.gb, a.t0);
+    collide(fr, gr, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+    a.phip[n] = (typename Codec<S>::P)m.phi;
+    scatter<S, SWAPPED, PERIODIC>(a, g, fr, gr, m.rho);
+}
+
+}  // namespace lbm

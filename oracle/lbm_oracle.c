@@ -1,0 +1,490 @@
+/*
+ * lbm_oracle.c — CPU oracle for the LBM-DDF Rayleigh–Bénard time step.
+ *
+ * TEST INFRASTRUCTURE ONLY (the checker, never the product; see lbm_oracle.h).
+ *
+ * Every function restates one piece of the reference single-GPU path of
+ * Summer536/LBM_DDF in FP64 and in the reference's operation order.  The
+ * compiler's own contraction is disabled (-ffp-contract=off, oracle/Makefile);
+ * the multiply-adds that nvcc fuses when it builds the reference are written
+ * out as fma() (the contraction model below), so the oracle reproduces the
+ * reference binary's results bit for bit: the fixtures under tests/golden/
+ * (1, 2, 50 and 1000 steps, two grids) match with zero differing bits.
+ */
+#include "lbm_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* D3Q27 velocity set in the reference's population order, src/initial.cu:71-73. */
+static const int CX[ORC_Q] = {0, 1, 0, -1, 0, 0, 0, 1, -1, -1, 1, 1, 0, -1,
+                              0, 1, 0, -1, 0, 1, -1, -1, 1, 1, -1, -1, 1};
+static const int CY[ORC_Q] = {0, 0, 1, 0, -1, 0, 0, 1, 1, -1, -1, 0, 1, 0,
+                              -1, 0, 1, 0, -1, 1, 1, -1, -1, 1, 1, -1, -1};
+static const int CZ[ORC_Q] = {0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, 1,
+                              1, -1, -1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1};
+
+/* Contraction model.  nvcc fuses a multiply that feeds an add or subtract
+ * into one FMA (one rounding) by default, and the reference is built that
+ * way.  Each place in the reference's step where it may do so is one bit
+ * below; a set bit computes that place with fma().  FUSE_NVCC is the set
+ * that reproduces the reference binary's outputs exactly: it was found by
+ * running every combination against the reference's own outputs (the
+ * fixtures under tests/golden/) and is the only one with zero differences
+ * after 1000 steps; nvcc leaves the force term's multiply-add unfused.  Mask 0
+ * rounds every operation separately, as the C source reads under strict
+ * IEEE evaluation. */
+enum {
+    FUSE_UV = 1 << 0,      /* u*u + v*v + w*w          (f and g collisions) */
+    FUSE_Q_F = 1 << 1,     /* eu*eu - uv               (f collision) */
+    FUSE_FEQ = 1 << 2,     /* f - w*(rho + ...)        (f collision) */
+    FUSE_FORCE = 1 << 3,   /* fchange + fc*feq_rho0    (f collision) */
+    FUSE_GEQ = 1 << 4,     /* g - (w*phi)*(1 + ...)    (g collision) */
+    FUSE_ABB = 1 << 5,     /* -g + (2 w T)*(1 + rho)   (anti-bounce-back) */
+    FUSE_Q_G = 1 << 6,     /* eu*eu - uv               (g collision) */
+};
+#define FUSE_NVCC (FUSE_UV | FUSE_Q_F | FUSE_FEQ | FUSE_GEQ | FUSE_ABB | FUSE_Q_G)
+static int orc_contract = FUSE_NVCC;
+
+void orc_set_contract(int mask) { orc_contract = mask; }
+int orc_get_contract(void) { return orc_contract; }
+
+/* a*b + c, fused (one rounding) when the site's bit is set */
+static inline double mad(int site, double a, double b, double c) {
+    return (orc_contract & site) ? fma(a, b, c) : a * b + c;
+}
+
+struct orc_state {
+    orc_params p;
+    int64_t n;
+    double *f, *g, *f_temp, *g_temp;
+    double *rho, *ux, *uy, *uz, *phi, *fx, *fy, *fz;
+    double w[ORC_Q];
+    int opp[ORC_Q];
+};
+
+/* Lattice weights, src/initial.cu:77-83. */
+static void orc_weights(double *w) {
+    for (int i = 0; i < ORC_Q; i++) {
+        if (i == 0)
+            w[i] = 8.0 / 27.0;
+        else if (i <= 6)
+            w[i] = 2.0 / 27.0;
+        else if (i <= 18)
+            w[i] = 1.0 / 54.0;
+        else
+            w[i] = 1.0 / 216.0;
+    }
+}
+
+static void orc_opposites(int *opp) {
+    for (int i = 0; i < ORC_Q; i++)
+        for (int j = 0; j < ORC_Q; j++)
+            if (CX[j] == -CX[i] && CY[j] == -CY[i] && CZ[j] == -CZ[i]) opp[i] = j;
+}
+
+int orc_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* src/globals.cu:13-23 (H = LY, the vertical node count). */
+int orc_derive(orc_params *p) {
+    if (p->lx < 2 || p->ly < 3 || p->lz < 2) return -1;
+    double ly = (double)p->ly;
+    p->visc = ly * sqrt(p->gravity * p->beta * (p->t_hot - p->t_cold) * ly * p->prandtl / p->rayleigh);
+    p->tau = 3.0 * p->visc + 0.5;
+    p->u0 = sqrt(p->gravity * p->beta * (p->t_hot - p->t_cold) * ly);
+    p->diff = p->visc / p->prandtl;
+    p->tauc = 3.0 * p->diff + 0.5;
+    p->t0 = 0.5 * (p->t_cold + p->t_hot);
+    return 0;
+}
+
+orc_state *orc_create(const orc_params *p) {
+    orc_params q = *p;
+    if (orc_derive(&q) != 0) return NULL;
+    orc_state *s = (orc_state *)calloc(1, sizeof(orc_state));
+    if (!s) return NULL;
+    s->p = q;
+    s->n = (int64_t)q.lx * q.ly * q.lz;
+    size_t big = (size_t)ORC_Q * (size_t)s->n * sizeof(double);
+    size_t one = (size_t)s->n * sizeof(double);
+    s->f = (double *)calloc(1, big);
+    s->g = (double *)calloc(1, big);
+    s->f_temp = (double *)calloc(1, big);
+    s->g_temp = (double *)calloc(1, big);
+    s->rho = (double *)calloc(1, one);
+    s->ux = (double *)calloc(1, one);
+    s->uy = (double *)calloc(1, one);
+    s->uz = (double *)calloc(1, one);
+    s->phi = (double *)calloc(1, one);
+    s->fx = (double *)calloc(1, one);
+    s->fy = (double *)calloc(1, one);
+    s->fz = (double *)calloc(1, one);
+    if (!s->f || !s->g || !s->f_temp || !s->g_temp || !s->rho || !s->ux || !s->uy || !s->uz ||
+        !s->phi || !s->fx || !s->fy || !s->fz) {
+        orc_destroy(s);
+        return NULL;
+    }
+    orc_weights(s->w);
+    orc_opposites(s->opp);
+    return s;
+}
+
+void orc_destroy(orc_state *s) {
+    if (!s) return;
+    free(s->f); free(s->g); free(s->f_temp); free(s->g_temp);
+    free(s->rho); free(s->ux); free(s->uy); free(s->uz); free(s->phi);
+    free(s->fx); free(s->fy); free(s->fz);
+    free(s);
+}
+
+const orc_params *orc_get_params(const orc_state *s) { return &s->p; }
+int64_t orc_nodes(const orc_state *s) { return s->n; }
+
+double *orc_field(orc_state *s, int which) {
+    switch (which) {
+    case 0: return s->f;
+    case 1: return s->g;
+    case 2: return s->rho;
+    case 3: return s->ux;
+    case 4: return s->uy;
+    case 5: return s->uz;
+    case 6: return s->phi;
+    case 7: return s->fx;
+    case 8: return s->fy;
+    case 9: return s->fz;
+    default: return NULL;
+    }
+}
+
+/* ---- kernels of the reference step, one loop nest each ---------------------- */
+
+/* src/macrovar.cu:36-47 */
+static void k_forcing(orc_state *s) {
+    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    const int64_t n = s->n;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < n; i++) {
+        s->fx[i] = 0.0;
+        s->fy[i] = gb * (s->phi[i] - t0);
+        s->fz[i] = 0.0;
+    }
+}
+
+/* src/collision.cu:3-33 (lines 34-49 compute a stress tensor that is discarded). */
+static void k_collide_f(orc_state *s) {
+    const double tau = s->p.tau;
+    const int64_t n = s->n;
+    double *f = s->f;
+#pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < n; idx++) {
+        double fy9 = s->fy[idx];
+        double rho9 = s->rho[idx];
+        double u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            double RT = 1.0 / 3.0;
+            /* c*u products are exact (c in {-1,0,1}), so fusing them changes nothing */
+            double eu = ((double)CX[ip] * u9 + (double)CY[ip] * v9 + (double)CZ[ip] * w9) / RT;
+            double uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;  /* (u*u + v*v + w*w) / RT */
+            double q = mad(FUSE_Q_F, eu, eu, -uv);                   /* eu*eu - uv */
+            double feq_in = rho9 + eu + 0.5 * q;
+            /* -(f - w*feq_in) / tau, the product fused into the subtraction */
+            double fchange = -mad(FUSE_FEQ, -s->w[ip], feq_in, f[ip * n + idx]) / tau;
+            double feq_rho0 = s->w[ip] * (1.0 + eu + 0.5 * q);
+            double fc = (1.0 - 0.5 / tau) * fy9 * ((double)CY[ip] - v9) / RT;
+            fchange = mad(FUSE_FORCE, fc, feq_rho0, fchange);        /* fchange += fc * feq_rho0 */
+            f[ip * n + idx] += fchange;
+        }
+    }
+}
+
+/* src/collision.cu:52-64 */
+static void k_collide_g(orc_state *s) {
+    const double tauc = s->p.tauc;
+    const int64_t n = s->n;
+    double *g = s->g;
+#pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < n; idx++) {
+        double phi9 = s->phi[idx];
+        double u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
+        double RT = 1.0 / 3.0;
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            double g9 = g[ip * n + idx];
+            double eu = ((double)CX[ip] * u9 + (double)CY[ip] * v9 + (double)CZ[ip] * w9) / RT;
+            double uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;
+            double geq_in = 1.0 + eu + 0.5 * mad(FUSE_Q_G, eu, eu, -uv);
+            /* -(g9 - (w*phi9)*geq_in) / tauc, the product fused into the subtraction */
+            double gchange = -mad(FUSE_GEQ, -(s->w[ip] * phi9), geq_in, g9) / tauc;
+            g[ip * n + idx] += gchange;
+        }
+    }
+}
+
+/* Pull streaming with wall rules, src/streaming.cu:3-125 (scalar = 0, field f)
+ * and :127-251 (scalar = 1, field g).
+ *
+ * Population k at node x is pulled from x - c_k.  When that source lies
+ * outside the box the reference applies, in the order x-, x+, y-, y+, z-, z+
+ * (:59-124, :183-250), the rule of each face the source is beyond; the last
+ * rule written wins.  Every rule for f and the x/z rules for g are halfway
+ * bounce-back, temp[k] = src[opp(k)] at the same node.  The y rules for g are
+ * anti-bounce-back, temp[k] = -src[opp(k)] + 2 w_k T_wall (1 + rho) with the
+ * rho of the previous macrovar (:205-228).  So for g: a source beyond a z face
+ * gives bounce-back, else beyond a y face gives anti-bounce-back, else
+ * bounce-back.  In periodic-side mode the x and z sources wrap instead. */
+static void k_stream(orc_state *s, int scalar) {
+    const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
+    const int per = s->p.periodic_sides;
+    const int64_t n = s->n;
+    const double *src = scalar ? s->g : s->f;
+    double *dst = scalar ? s->g_temp : s->f_temp;
+    const double t_hot = s->p.t_hot, t_cold = s->p.t_cold;
+#pragma omp parallel for schedule(static)
+    for (int iz = 0; iz < lz; iz++) {
+        for (int iy = 0; iy < ly; iy++) {
+            for (int ix = 0; ix < lx; ix++) {
+                int64_t idx = ((int64_t)iz * ly + iy) * lx + ix;
+                for (int k = 0; k < ORC_Q; k++) {
+                    int sx = ix - CX[k], sy = iy - CY[k], sz = iz - CZ[k];
+                    int out_x = 0, out_z = 0;
+                    if (per) {
+                        sx = (sx + lx) % lx;
+                        sz = (sz + lz) % lz;
+                    } else {
+                        out_x = (sx < 0 || sx >= lx);
+                        out_z = (sz < 0 || sz >= lz);
+                    }
+                    int out_y = (sy < 0 || sy >= ly);
+                    if (!out_x && !out_y && !out_z) {
+                        int64_t sidx = ((int64_t)sz * ly + sy) * lx + sx;
+                        dst[k * n + idx] = src[k * n + sidx];
+                        continue;
+                    }
+                    double back = src[(int64_t)s->opp[k] * n + idx];
+                    if (scalar && out_y && !out_z) {
+                        double density = s->rho[idx];
+                        double tw = (sy < 0) ? t_hot : t_cold;
+                        dst[k * n + idx] = mad(FUSE_ABB, 2.0 * s->w[k] * tw, 1.0 + density, -back);
+                    } else {
+                        dst[k * n + idx] = back;
+                    }
+                }
+            }
+        }
+    }
+}
+
+/* src/macrovar.cu:3-34 */
+static void k_macrovar(orc_state *s) {
+    const int64_t n = s->n;
+#pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < n; idx++) {
+        double rho_l = 0.0, ux_l = 0.0, uy_l = 0.0, uz_l = 0.0, phi_l = 0.0;
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            double f_val = s->f[ip * n + idx];
+            double g_val = s->g[ip * n + idx];
+            rho_l += f_val;
+            ux_l += (double)CX[ip] * f_val;
+            uy_l += (double)CY[ip] * f_val;
+            uz_l += (double)CZ[ip] * f_val;
+            phi_l += g_val;
+        }
+        s->rho[idx] = rho_l;
+        s->ux[idx] = ux_l + 0.5 * s->fx[idx];
+        s->uy[idx] = uy_l + 0.5 * s->fy[idx];
+        s->uz[idx] = uz_l + 0.5 * s->fz[idx];
+        s->phi[idx] = phi_l;
+    }
+}
+
+void orc_step(orc_state *s, int nsteps) {
+    size_t bytes = (size_t)ORC_Q * (size_t)s->n * sizeof(double);
+    for (int it = 0; it < nsteps; it++) {
+        k_forcing(s);          /* src/main.cu:27 */
+        k_collide_f(s);        /* :29 */
+        k_collide_g(s);        /* :33 */
+        k_stream(s, 0);        /* :38 */
+        memcpy(s->f, s->f_temp, bytes);   /* :39 */
+        k_stream(s, 1);        /* :40 */
+        memcpy(s->g, s->g_temp, bytes);   /* :41 */
+        k_macrovar(s);         /* :45 */
+    }
+}
+
+/* ---- initial states ---------------------------------------------------------- */
+
+/* src/initial.cu:208-241 */
+void orc_init_rest(orc_state *s) {
+    const int64_t n = s->n;
+    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    for (int64_t idx = 0; idx < n; idx++) {
+        s->rho[idx] = 0.0;
+        s->ux[idx] = 0.0;
+        s->uy[idx] = 0.0;
+        s->uz[idx] = 0.0;
+        s->phi[idx] = 0.5;
+        s->fx[idx] = 0.0;
+        s->fy[idx] = gb * (s->phi[idx] - t0);
+        s->fz[idx] = 0.0;
+        double usq = 0.0;
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            double feq = s->w[ip] * s->rho[idx] * (1.0 - 1.5 * usq);
+            s->f[ip * n + idx] = feq - 0.5 * s->fy[idx] * (double)CY[ip] / (1.0 / 3.0) * feq;
+            double geq = s->w[ip] * s->phi[idx] * (1.0 - 1.5 * usq);
+            s->g[ip * n + idx] = geq;
+        }
+    }
+}
+
+/* splitmix64 finaliser (Steele, Lea & Flood 2014; constants as published by Vigna). */
+static uint64_t splitmix64(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    x = (x ^ (x >> 30)) * 0xBF58476D1CE4E5B9ull;
+    x = (x ^ (x >> 27)) * 0x94D049BB133111EBull;
+    return x ^ (x >> 31);
+}
+
+double orc_noise_uniform(uint64_t seed, uint64_t node) {
+    uint64_t r = splitmix64(splitmix64(seed) + node);
+    return (double)(r >> 11) * (1.0 / 9007199254740992.0);
+}
+
+void orc_set_populations(orc_state *s, const double *f, const double *g, const double *phi_prev) {
+    const int64_t n = s->n;
+    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    memcpy(s->f, f, (size_t)ORC_Q * (size_t)n * sizeof(double));
+    memcpy(s->g, g, (size_t)ORC_Q * (size_t)n * sizeof(double));
+    for (int64_t i = 0; i < n; i++) {
+        double pp = phi_prev ? phi_prev[i] : t0;
+        s->fx[i] = 0.0;
+        s->fy[i] = gb * (pp - t0);
+        s->fz[i] = 0.0;
+    }
+    k_macrovar(s);
+}
+
+void orc_init_conduction(orc_state *s, uint64_t seed, double amplitude) {
+    const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
+    const int64_t n = s->n;
+    double *f = (double *)calloc((size_t)ORC_Q * (size_t)n, sizeof(double));
+    double *g = (double *)malloc((size_t)ORC_Q * (size_t)n * sizeof(double));
+    double *pp = (double *)malloc((size_t)n * sizeof(double));
+    if (!f || !g || !pp) {
+        free(f); free(g); free(pp);
+        return;
+    }
+    for (int iz = 0; iz < lz; iz++)
+        for (int iy = 0; iy < ly; iy++)
+            for (int ix = 0; ix < lx; ix++) {
+                int64_t idx = ((int64_t)iz * ly + iy) * lx + ix;
+                double u = orc_noise_uniform(seed, (uint64_t)idx);
+                double t = s->p.t_hot - (s->p.t_hot - s->p.t_cold) * (double)iy / ((double)ly - 1.0);
+                t = t + amplitude * (2.0 * u - 1.0);
+                pp[idx] = t;
+                for (int ip = 0; ip < ORC_Q; ip++) g[ip * n + idx] = s->w[ip] * t;
+            }
+    orc_set_populations(s, f, g, pp);
+    free(f); free(g); free(pp);
+}
+
+/* src/initial.cu:110-205: the restart reader copies all seven arrays, then
+ * launches forcing (:202). */
+void orc_load_restart(orc_state *s, const double *rho, const double *ux, const double *uy,
+                      const double *uz, const double *phi, const double *f, const double *g) {
+    const size_t one = (size_t)s->n * sizeof(double);
+    memcpy(s->rho, rho, one);
+    memcpy(s->ux, ux, one);
+    memcpy(s->uy, uy, one);
+    memcpy(s->uz, uz, one);
+    memcpy(s->phi, phi, one);
+    memcpy(s->f, f, (size_t)ORC_Q * one);
+    memcpy(s->g, g, (size_t)ORC_Q * one);
+    k_forcing(s);
+}
+
+/* ---- diagnostics --------------------------------------------------------------- */
+
+void orc_observables(const orc_state *s, double out[10]) {
+    const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
+    const int64_t n = s->n;
+    const double dT = s->p.t_hot - s->p.t_cold;
+    /* Nu_bulk, src/output.cu:199-201, 228-233 */
+    double uyT = 0.0;
+    for (int64_t i = 0; i < n; i++) uyT += s->uy[i] * s->phi[i];
+    uyT /= (double)n;
+    out[0] = 1.0 + uyT * (double)ly / (s->p.diff * dT);
+    /* Nu_top / Nu_bottom from the one-sided plate gradients, :203-256 */
+    double top = 0.0, bot = 0.0;
+    int64_t cnt = 0;
+    for (int ix = 0; ix < lx; ix++)
+        for (int iz = 0; iz < lz; iz++) {
+            const double *p = s->phi;
+            int64_t b0 = ((int64_t)iz * ly + 0) * lx + ix;
+            int64_t b1 = ((int64_t)iz * ly + 1) * lx + ix;
+            int64_t b2 = ((int64_t)iz * ly + 2) * lx + ix;
+            int64_t t0 = ((int64_t)iz * ly + (ly - 1)) * lx + ix;
+            int64_t t1 = ((int64_t)iz * ly + (ly - 2)) * lx + ix;
+            int64_t t2 = ((int64_t)iz * ly + (ly - 3)) * lx + ix;
+            top += (3.0 * p[t0] - 4.0 * p[t1] + p[t2]) / 2.0;
+            bot += (-3.0 * p[b0] + 4.0 * p[b1] - p[b2]) / 2.0;
+            cnt++;
+        }
+    top /= (double)cnt;
+    bot /= (double)cnt;
+    out[1] = -top * (double)ly / dT;
+    out[2] = -bot * (double)ly / dT;
+    /* kinetic energy, Reynolds number, means, finiteness */
+    double usq = 0.0, mx = 0.0, my = 0.0, mz = 0.0, mt = 0.0;
+    int bad = 0;
+    for (int64_t i = 0; i < n; i++) {
+        double a = s->ux[i], b = s->uy[i], c = s->uz[i], t = s->phi[i];
+        usq += a * a + b * b + c * c;
+        mx += a;
+        my += b;
+        mz += c;
+        mt += t;
+        if (!isfinite(a) || !isfinite(b) || !isfinite(c) || !isfinite(t) || !isfinite(s->rho[i])) bad = 1;
+    }
+    usq /= (double)n;
+    out[3] = 0.5 * usq;
+    out[4] = sqrt(usq) * (double)ly / s->p.visc;
+    out[5] = mx / (double)n;
+    out[6] = my / (double)n;
+    out[7] = mz / (double)n;
+    out[8] = mt / (double)n;
+    out[9] = bad ? 1.0 : 0.0;
+}
+
+/* src/output.cu:336-368 */
+void orc_profile(const orc_state *s, double *out) {
+    const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
+    for (int iy = 0; iy < ly; iy++) {
+        double sx = 0.0, sy = 0.0, sz = 0.0, sp = 0.0, sp2 = 0.0;
+        int64_t count = 0;
+        for (int ix = 0; ix < lx; ix++)
+            for (int iz = 0; iz < lz; iz++) {
+                int64_t idx = ((int64_t)iz * ly + iy) * lx + ix;
+                sx += s->ux[idx];
+                sy += s->uy[idx];
+                sz += s->uz[idx];
+                sp += s->phi[idx];
+                sp2 += s->phi[idx] * s->phi[idx];
+                count++;
+            }
+        double ap = sp / (double)count;
+        out[5 * iy + 0] = sx / (double)count;
+        out[5 * iy + 1] = sy / (double)count;
+        out[5 * iy + 2] = sz / (double)count;
+        out[5 * iy + 3] = ap;
+        out[5 * iy + 4] = sqrt(sp2 / (double)count - ap * ap);
+    }
+}

@@ -1,0 +1,188 @@
+"""ctypes view of the CPU oracle (oracle/liblbm_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: the parity tests, ``__graft_entry__.smoke()`` and
+``bench.py``'s cpu_baseline / reference legs use this module as the checker.
+The product package ``lbm_ddf_b200`` never imports it.
+
+The oracle restates the reference single-GPU step (Summer536/LBM_DDF ``src/``)
+in FP64; see ``oracle/lbm_oracle.h`` for the per-function citations.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liblbm_oracle.so")
+
+Q = 27
+# D3Q27 order of src/initial.cu:71-73
+CX = np.array([0, 1, 0, -1, 0, 0, 0, 1, -1, -1, 1, 1, 0, -1, 0, 1, 0, -1, 0, 1, -1, -1, 1, 1, -1, -1, 1])
+CY = np.array([0, 0, 1, 0, -1, 0, 0, 1, 1, -1, -1, 0, 1, 0, -1, 0, 1, 0, -1, 1, 1, -1, -1, 1, 1, -1, -1])
+CZ = np.array([0, 0, 0, 0, 0, 1, -1, 0, 0, 0, 0, 1, 1, 1, 1, -1, -1, -1, -1, 1, 1, 1, 1, -1, -1, -1, -1])
+W = np.array([8.0 / 27.0] + [2.0 / 27.0] * 6 + [1.0 / 54.0] * 12 + [1.0 / 216.0] * 8)
+
+
+class OrcParams(C.Structure):
+    _fields_ = [
+        ("lx", C.c_int32), ("ly", C.c_int32), ("lz", C.c_int32),
+        ("periodic_sides", C.c_int32),
+        ("rayleigh", C.c_double), ("prandtl", C.c_double),
+        ("t_hot", C.c_double), ("t_cold", C.c_double),
+        ("gravity", C.c_double), ("beta", C.c_double),
+        ("visc", C.c_double), ("tau", C.c_double), ("u0", C.c_double),
+        ("diff", C.c_double), ("tauc", C.c_double), ("t0", C.c_double),
+    ]
+
+
+_lib = None
+
+
+def build() -> str:
+    """Compile the oracle with oracle/Makefile (gcc, OpenMP, no FP contraction)."""
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        P = C.POINTER(OrcParams)
+        dp = C.POINTER(C.c_double)
+        L.orc_derive.argtypes = [P]
+        L.orc_derive.restype = C.c_int
+        L.orc_create.argtypes = [P]
+        L.orc_create.restype = C.c_void_p
+        L.orc_destroy.argtypes = [C.c_void_p]
+        L.orc_nodes.argtypes = [C.c_void_p]
+        L.orc_nodes.restype = C.c_int64
+        L.orc_field.argtypes = [C.c_void_p, C.c_int]
+        L.orc_field.restype = dp
+        L.orc_init_rest.argtypes = [C.c_void_p]
+        L.orc_init_conduction.argtypes = [C.c_void_p, C.c_uint64, C.c_double]
+        L.orc_noise_uniform.argtypes = [C.c_uint64, C.c_uint64]
+        L.orc_noise_uniform.restype = C.c_double
+        L.orc_set_populations.argtypes = [C.c_void_p, dp, dp, dp]
+        L.orc_load_restart.argtypes = [C.c_void_p] + [dp] * 7
+        L.orc_step.argtypes = [C.c_void_p, C.c_int]
+        L.orc_observables.argtypes = [C.c_void_p, dp]
+        L.orc_profile.argtypes = [C.c_void_p, dp]
+        L.orc_threads.restype = C.c_int
+        L.orc_set_contract.argtypes = [C.c_int]
+        L.orc_get_contract.restype = C.c_int
+        _lib = L
+    return _lib
+
+
+def _dp(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+FIELDS = {"f": 0, "g": 1, "rho": 2, "ux": 3, "uy": 4, "uz": 5, "phi": 6,
+          "force_x": 7, "force_y": 8, "force_z": 9}
+
+
+def make_params(lx, ly, lz, rayleigh=1e5, prandtl=0.71, t_hot=1.0, t_cold=0.0,
+                gravity=1.0, beta=None, periodic_sides=False) -> OrcParams:
+    """Run-surface fields of src/parameters.h:8-26.  beta=None picks the
+    free-fall velocity 0.1, i.e. beta = 0.01 / (gravity * dT * LY)."""
+    if beta is None:
+        beta = 0.01 / (gravity * (t_hot - t_cold) * ly)
+    p = OrcParams(lx=lx, ly=ly, lz=lz, periodic_sides=int(bool(periodic_sides)),
+                  rayleigh=rayleigh, prandtl=prandtl, t_hot=t_hot, t_cold=t_cold,
+                  gravity=gravity, beta=beta)
+    if lib().orc_derive(C.byref(p)) != 0:
+        raise ValueError("bad grid for the oracle")
+    return p
+
+
+class Oracle:
+    """One reference-layout FP64 case on the CPU."""
+
+    def __init__(self, params: OrcParams):
+        self.params = params
+        self._h = lib().orc_create(C.byref(params))
+        if not self._h:
+            raise MemoryError("orc_create failed")
+        self.n = int(lib().orc_nodes(self._h))
+        self.shape = (params.lz, params.ly, params.lx)
+
+    def close(self):
+        if self._h:
+            lib().orc_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def field(self, name: str) -> np.ndarray:
+        """Live numpy view of a field (f and g are (27, LZ, LY, LX))."""
+        ptr = lib().orc_field(self._h, FIELDS[name])
+        count = self.n * (Q if name in ("f", "g") else 1)
+        a = np.ctypeslib.as_array(ptr, shape=(count,))
+        return a.reshape((Q,) + self.shape if name in ("f", "g") else self.shape)
+
+    def init_rest(self):
+        lib().orc_init_rest(self._h)
+
+    def init_conduction(self, seed: int, amplitude: float = 1e-3):
+        lib().orc_init_conduction(self._h, C.c_uint64(seed), amplitude)
+
+    def set_populations(self, f, g, phi_prev=None):
+        f = np.ascontiguousarray(f, dtype=np.float64)
+        g = np.ascontiguousarray(g, dtype=np.float64)
+        pp = None if phi_prev is None else _dp(np.ascontiguousarray(phi_prev, dtype=np.float64))
+        lib().orc_set_populations(self._h, _dp(f), _dp(g), pp)
+
+    def load_restart(self, rho, ux, uy, uz, phi, f, g):
+        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, uz, phi, f, g)]
+        lib().orc_load_restart(self._h, *[_dp(a) for a in arrs])
+
+    def step(self, n: int = 1):
+        lib().orc_step(self._h, int(n))
+
+    def observables(self) -> dict:
+        out = np.zeros(10)
+        lib().orc_observables(self._h, _dp(out))
+        keys = ["nu_bulk", "nu_top", "nu_bottom", "ke", "re", "ux_mean", "uy_mean",
+                "uz_mean", "phi_mean", "diverged"]
+        return dict(zip(keys, out.tolist()))
+
+    def profile(self) -> np.ndarray:
+        out = np.zeros(5 * self.params.ly)
+        lib().orc_profile(self._h, _dp(out))
+        return out.reshape(self.params.ly, 5)
+
+
+NVCC_FUSION = None  # the default mask, read from the library on first use
+
+
+def set_contract(mask) -> None:
+    """Rounding model: a bit mask of fused multiply-add sites (lbm_oracle.c);
+    True selects the mask that rounds as the nvcc-built reference does,
+    False / 0 rounds every operation separately."""
+    global NVCC_FUSION
+    if NVCC_FUSION is None:
+        NVCC_FUSION = get_contract()
+    if mask is True:
+        mask = NVCC_FUSION
+    lib().orc_set_contract(int(mask))
+
+
+def get_contract() -> int:
+    return int(lib().orc_get_contract())
+
+
+def threads() -> int:
+    return int(lib().orc_threads())
+
+
+def noise_uniform(seed: int, node: int) -> float:
+    return float(lib().orc_noise_uniform(C.c_uint64(seed), C.c_uint64(node)))

@@ -1,0 +1,33 @@
+"""Cases the reference program is built for (oracle/build_ref.py) and run on
+(tests/golden/make_golden.py, bench.py's reference arm).  TEST INFRASTRUCTURE.
+
+Every case uses T_hot = 1, T_cold = 0, gravity 1 and beta = 0.01/LY (free-fall
+velocity 0.1).  continue_step > 0 makes the reference start from restart files
+(src/initial.cu:110-205), which is how seeded states are fed to it.
+"""
+NEVER = 1_000_000_000
+
+REF_CASES = {
+    # parity cases on small non-cubic closed boxes
+    "w12_rest50": dict(lx=12, ly=10, lz=8, continue_step=0, nend=50, ndiag=10, nnuout=10,
+                       rayleigh=1.0e5, prandtl=0.71),
+    "w12_s1": dict(lx=12, ly=10, lz=8, continue_step=100, nend=101, rayleigh=1.0e5, prandtl=0.71),
+    "w12_s2": dict(lx=12, ly=10, lz=8, continue_step=100, nend=102, rayleigh=1.0e5, prandtl=0.71),
+    "w12_s1000": dict(lx=12, ly=10, lz=8, continue_step=100, nend=1100, ndiag=100, nnuout=100,
+                      rayleigh=1.0e5, prandtl=0.71),
+    "w24_s1000": dict(lx=24, ly=16, lz=20, continue_step=100, nend=1100, ndiag=100, nnuout=100,
+                      rayleigh=1.0e5, prandtl=0.71),
+    # timing cases: 256^3, Ra 1e7 (and 64^3, Ra 1e5) from the rest state
+    "c1_n3": dict(lx=256, ly=256, lz=256, continue_step=0, nend=3, rayleigh=1.0e7, prandtl=0.71),
+    "c1_n53": dict(lx=256, ly=256, lz=256, continue_step=0, nend=53, rayleigh=1.0e7, prandtl=0.71),
+    "c1_n103": dict(lx=256, ly=256, lz=256, continue_step=0, nend=103, rayleigh=1.0e7, prandtl=0.71),
+    "c1_n203": dict(lx=256, ly=256, lz=256, continue_step=0, nend=203, rayleigh=1.0e7, prandtl=0.71),
+    "c0_n3": dict(lx=64, ly=64, lz=64, continue_step=0, nend=3, rayleigh=1.0e5, prandtl=0.71),
+    "c0_n203": dict(lx=64, ly=64, lz=64, continue_step=0, nend=203, rayleigh=1.0e5, prandtl=0.71),
+}
+
+# timing binaries of one grid: (grid tag, warm-up NEND, [longer NEND ...])
+TIMING_SETS = {
+    "c1": (3, [53, 103, 203]),
+    "c0": (3, [203]),
+}

@@ -1,0 +1,267 @@
+"""Parity of the CUDA engine (through the C ABI) with the reference's outputs
+and with the CPU oracle.
+
+Tolerances (field-relative, max|a-b| / max|b|):
+  FP64 storage      populations 1e-12, macroscopic fields 1e-12, Nu 1e-10
+  FP32 storage      5e-5 after <= 200 steps (FP32 arithmetic)
+  FP16S / BF16S     5e-3 / 4e-2 after <= 100 steps (16-bit storage)
+"""
+import hashlib
+
+import numpy as np
+import pytest
+
+from helpers import load_golden, nu_from_fields, relerr
+from oracle.ref_cases import REF_CASES
+
+pytestmark = pytest.mark.gpu
+
+FIELDS = ("f", "g", "rho", "ux", "uy", "uz", "phi")
+
+
+@pytest.fixture(scope="module", autouse=True)
+def _need_gpu():
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+
+
+def engine_run(lbm, params, steps, seed=None, amplitude=1e-3, state=None, rest=False, chunks=None):
+    with lbm.Case(params) as c:
+        if state is not None:
+            c.load_ref_state(*(state[k] for k in ("rho", "ux", "uy", "uz", "phi", "f", "g")))
+        elif rest:
+            c.init_rest()
+        else:
+            c.init_conduction(seed, amplitude)
+        for n in (chunks or [steps]):
+            c.step(n)
+        out = c.store_ref_state()
+        out["obs"] = c.observables()
+        out["profile"] = c.profile()
+        assert c.step_count == steps
+    return out
+
+
+def oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=None, amplitude=1e-3, rest=False, ra=1e5, pr=0.71):
+    o = oracle_mod.Oracle(oracle_mod.make_params(lx, ly, lz, rayleigh=ra, prandtl=pr, periodic_sides=periodic))
+    if rest:
+        o.init_rest()
+    else:
+        o.init_conduction(seed, amplitude)
+    o.step(steps)
+    return o
+
+
+def compare(got, o, tol, fields=FIELDS):
+    for k in fields:
+        e = relerr(got[k].reshape(-1), o.field(k).reshape(-1))
+        assert e <= tol, f"{k}: {e:.3e} > {tol:.1e}"
+
+
+# ---------------------------------------------------------------- reference
+
+@pytest.mark.parametrize("name", ["w12_s1", "w12_s2", "w12_rest50", "w12_s1000", "w24_s1000"])
+def test_f64_matches_reference_outputs(lbm, oracle_mod, name):
+    """FP64 engine, closed box, fed the same state the reference was fed
+    (its restart files), against what the reference wrote at NEND."""
+    g = load_golden(name)
+    c = REF_CASES[name]
+    steps = int(g["steps"])
+    p = lbm.make_params(c["lx"], c["ly"], c["lz"], rayleigh=c["rayleigh"], prandtl=c["prandtl"],
+                        sides=lbm.SIDES_WALL, storage="f64")
+    if c["continue_step"] == 0:
+        got = engine_run(lbm, p, steps, rest=True)
+    else:
+        o = oracle_mod.Oracle(oracle_mod.make_params(c["lx"], c["ly"], c["lz"], rayleigh=c["rayleigh"],
+                                                     prandtl=c["prandtl"]))
+        o.init_conduction(int(g["seed"]), float(g["amplitude"]))
+        st = {k: o.field(k).copy() for k in FIELDS}
+        h = hashlib.sha256()
+        for k in ("rho", "ux", "uy", "uz", "phi", "f", "g"):
+            h.update(np.ascontiguousarray(st[k]).tobytes())
+        assert h.hexdigest() == str(g["input_sha256"])
+        got = engine_run(lbm, p, steps, state=st)
+    n = c["lx"] * c["ly"] * c["lz"]
+    for k in ("f", "g"):
+        a = got[k].reshape(27, n)
+        if "sample_nodes" in g:
+            a = a[:, g["sample_nodes"]]
+        assert relerr(a.reshape(-1), g[k].reshape(-1)) <= 1e-12, k
+    for k in ("rho", "ux", "uy", "uz", "phi"):
+        assert relerr(got[k].reshape(-1), g[k]) <= 1e-12, k
+    d = lbm.derive(p)
+    ref_nu = nu_from_fields(g["uy"], g["phi"], c["lx"], c["ly"], c["lz"], d["diff"])
+    eng = (got["obs"]["nu_bulk"], got["obs"]["nu_top"], got["obs"]["nu_bottom"])
+    for a, b in zip(eng, ref_nu):
+        assert abs(a - b) <= 1e-10 * max(1.0, abs(b))
+
+
+# ---------------------------------------------------------------- oracle, FP64
+
+def test_f64_init_is_bitwise_the_oracles(lbm, oracle_mod):
+    lx, ly, lz = 20, 14, 9
+    for periodic in (True, False):
+        p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
+        got = engine_run(lbm, p, 0, seed=99)
+        o = oracle_run(oracle_mod, lx, ly, lz, 0, periodic, seed=99)
+        for k in FIELDS:
+            assert np.array_equal(got[k].reshape(-1), o.field(k).reshape(-1)), k
+
+
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("steps", [1, 2, 3, 10, 101])
+def test_f64_matches_oracle(lbm, oracle_mod, periodic, steps):
+    lx, ly, lz = 20, 14, 9
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
+    got = engine_run(lbm, p, steps, seed=5)
+    o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=5)
+    compare(got, o, 1e-12)
+    ob = o.observables()
+    for k in ("nu_bulk", "nu_top", "nu_bottom", "ke", "re", "phi_mean"):
+        assert abs(got["obs"][k] - ob[k]) <= 1e-10 * max(1.0, abs(ob[k])), k
+    for k in ("ux_mean", "uy_mean", "uz_mean"):
+        assert abs(got["obs"][k] - ob[k]) <= 1e-14, k
+    np.testing.assert_allclose(got["profile"], o.profile(), rtol=1e-11, atol=1e-15)
+
+
+def test_f64_step_chunking_is_irrelevant(lbm):
+    """7 steps in one call equals 3 + 1 + 3 calls (layout flag bookkeeping)."""
+    p = lbm.make_params(16, 12, 10, sides=lbm.SIDES_WALL, storage="f64")
+    a = engine_run(lbm, p, 7, seed=1)
+    b = engine_run(lbm, p, 7, seed=1, chunks=[3, 1, 3])
+    for k in FIELDS:
+        assert np.array_equal(a[k], b[k]), k
+
+
+def test_f64_larger_box_vs_oracle(lbm, oracle_mod):
+    lx, ly, lz, steps = 96, 64, 80, 3
+    for periodic in (True, False):
+        p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
+        got = engine_run(lbm, p, steps, seed=11)
+        o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=11)
+        compare(got, o, 1e-12)
+
+
+def test_load_store_roundtrip(lbm, oracle_mod):
+    lx, ly, lz = 12, 10, 8
+    o = oracle_run(oracle_mod, lx, ly, lz, 5, False, seed=3)
+    st = {k: o.field(k).copy() for k in FIELDS}
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_WALL, storage="f64")
+    got = engine_run(lbm, p, 0, state=st)
+    for k in ("f", "g", "rho", "uy", "phi"):
+        assert relerr(got[k].reshape(-1), st[k].reshape(-1)) <= 1e-15, k
+
+
+def test_xz_mirror_symmetry(lbm):
+    """A state symmetric under x <-> z stays symmetric (D3Q27 is)."""
+    from oracle.oracle import CX, CY, CZ, W
+
+    lx = lz = 12
+    ly = 10
+    n = lx * ly * lz
+    rng = np.random.default_rng(4)
+    t = (1.0 - np.arange(ly) / (ly - 1.0))[None, :, None] + np.zeros((lz, ly, lx))
+    noise = rng.uniform(-1e-3, 1e-3, size=(lz, ly, lx))
+    noise = 0.5 * (noise + noise.transpose(2, 1, 0))
+    t = t + noise
+    g = W[:, None, None, None] * t[None]
+    f = np.zeros_like(g)
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_WALL, storage="f64")
+    uy = 0.5 * p.gravity * p.beta * (t - 0.5)
+    st = dict(rho=np.zeros(n), ux=np.zeros(n), uy=uy, uz=np.zeros(n), phi=t, f=f, g=g)
+    got = engine_run(lbm, p, 40, state=st)
+    # population i at (z, y, x) mirrors population swap(i) at (x, y, z)
+    swap = [int(np.where((CX == CZ[i]) & (CY == CY[i]) & (CZ == CX[i]))[0][0]) for i in range(27)]
+    fs = got["f"][swap].transpose(0, 3, 2, 1)
+    assert relerr(fs, got["f"]) <= 1e-12
+    assert relerr(got["phi"].transpose(2, 1, 0), got["phi"]) <= 1e-12
+
+
+def test_mass_is_conserved(lbm):
+    """sum(rho) is invariant under BGK + forcing + bounce-back."""
+    p = lbm.make_params(48, 32, 40, sides=lbm.SIDES_WALL, storage="f64")
+    with lbm.Case(p) as c:
+        c.init_conduction(8, 1e-2)
+        m0 = c.store_ref_state(("rho",))["rho"].sum()
+        c.step(200)
+        m1 = c.store_ref_state(("rho",))["rho"].sum()
+    assert abs(m1 - m0) < 1e-13
+
+
+# ---------------------------------------------------------------- reduced precision
+
+@pytest.mark.parametrize("storage,tol,steps", [("f32", 5e-5, 200), ("f16s", 5e-3, 100), ("bf16s", 4e-2, 100)])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_reduced_precision_vs_oracle(lbm, oracle_mod, storage, tol, steps, periodic):
+    lx, ly, lz = 24, 20, 16
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage=storage)
+    got = engine_run(lbm, p, steps, seed=21, amplitude=1e-2)
+    o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=21, amplitude=1e-2)
+    compare(got, o, tol, fields=("f", "g", "phi", "uy"))
+    ob = o.observables()
+    assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= 50 * tol
+
+
+# ---------------------------------------------------------------- failure detection
+
+def test_nan_in_state_is_reported(lbm, oracle_mod):
+    """Divergence injected on the host (a NaN in the loaded state) comes back
+    as LBM_ERR_DIVERGED from the observables call."""
+    lx, ly, lz = 12, 10, 8
+    o = oracle_run(oracle_mod, lx, ly, lz, 0, False, seed=2)
+    st = {k: o.field(k).copy() for k in FIELDS}
+    st["g"][3, 4, 5, 6] = np.nan
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_WALL, storage="f32")
+    with lbm.Case(p) as c:
+        c.load_ref_state(*(st[k] for k in ("rho", "ux", "uy", "uz", "phi", "f", "g")))
+        c.step(3)
+        with pytest.raises(lbm.LbmError) as e:
+            c.observables()
+        assert e.value.code == lbm.ERR_DIVERGED
+        assert c.observables(allow_diverged=True)["diverged"] == 1
+
+
+def test_step_before_init_is_an_error(lbm):
+    p = lbm.make_params(8, 8, 8)
+    with lbm.Case(p) as c:
+        with pytest.raises(lbm.LbmError) as e:
+            c.step(1)
+        assert e.value.code == lbm.ERR_STATE
+
+
+def test_torch_stream(lbm):
+    import torch
+
+    p = lbm.make_params(32, 24, 16, storage="f32")
+    s = torch.cuda.Stream()
+    with lbm.Case(p) as c:
+        c.init_conduction(1, stream=s)
+        c.step(10, stream=s)
+        a = c.observables(stream=s)
+    b = engine_run(lbm, p, 10, seed=1)["obs"]
+    assert a["nu_bulk"] == b["nu_bulk"]
+
+
+# ---------------------------------------------------------------- full size properties
+
+def test_full_size_256_f32_properties(lbm):
+    """At the 256^3 benchmark size (oracle too slow there): FP32 and FP64
+    engines agree after 20 steps, total mass is conserved, no NaN."""
+    p32 = lbm.make_params(256, 256, 256, rayleigh=1e7, sides=lbm.SIDES_PERIODIC, storage="f32")
+    p64 = lbm.make_params(256, 256, 256, rayleigh=1e7, sides=lbm.SIDES_PERIODIC, storage="f64")
+    res = {}
+    for name, p in (("f32", p32), ("f64", p64)):
+        with lbm.Case(p) as c:
+            c.init_conduction(42, 1e-3)
+            m0 = float(c.store_ref_state(("rho",))["rho"].sum())
+            c.step(20)
+            st = c.store_ref_state(("rho", "uy", "phi"))
+            res[name] = (st, c.observables(), m0, float(st["rho"].sum()))
+    (s32, o32, m0_32, m1_32), (s64, o64, m0_64, m1_64) = res["f32"], res["f64"]
+    assert abs(m1_64 - m0_64) < 1e-9
+    assert abs(m1_32 - m0_32) < 1e-2
+    assert relerr(s32["phi"], s64["phi"]) < 1e-5
+    assert relerr(s32["uy"], s64["uy"]) < 1e-3
+    assert abs(o32["nu_bulk"] - o64["nu_bulk"]) < 1e-4
