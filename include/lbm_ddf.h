@@ -160,6 +160,13 @@ int lbm_checkpoint_bytes(const lbm_case *c, uint64_t *bytes);
 int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream);
 int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *stream);
 
+/* Device self-check of the division identity the FP64 path uses for its
+ * constant divisors (a / b from the correctly rounded reciprocal with one
+ * Markstein correction): counts, over n random dividends, the results that
+ * differ from the GPU's correctly rounded division by `divisor`.  A
+ * diagnostic with no counterpart in the reference; expected result 0. */
+int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed, uint64_t *mismatches);
+
 /* Parameters and step count of a case. */
 int lbm_get_params(const lbm_case *c, lbm_params *p, lbm_derived *d, int64_t *step);
 

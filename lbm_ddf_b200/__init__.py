@@ -99,10 +99,11 @@ def lib() -> C.CDLL:
         L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
         L.lbm_save_state.argtypes = [vp, vp, C.c_uint64, vp]
         L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
+        L.lbm_selfcheck_division.argtypes = [C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
         for name in ("lbm_derive", "lbm_case_bytes", "lbm_create", "lbm_destroy", "lbm_init_rest",
                      "lbm_init_conduction", "lbm_load_ref_state", "lbm_store_ref_state", "lbm_step",
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
-                     "lbm_save_state", "lbm_restore_state"):
+                     "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -185,6 +186,14 @@ def derive(p: LbmParams) -> dict:
     d = LbmDerived()
     check(lib().lbm_derive(C.byref(p), C.byref(d)))
     return {k: getattr(d, k) for k, _ in d._fields_}
+
+
+def selfcheck_division(divisor: float, n: int = 1 << 24, seed: int = 1, device: int = 0) -> int:
+    """Mismatches of the FP64 path's division by `divisor` against the GPU's
+    correctly rounded division over n random dividends (expected 0)."""
+    bad = C.c_uint64()
+    check(lib().lbm_selfcheck_division(device, divisor, n, seed, C.byref(bad)))
+    return int(bad.value)
 
 
 def case_bytes(p: LbmParams) -> int:

@@ -84,7 +84,7 @@ __global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, d
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
         gather<S, SWAPPED>(a, g, fr, gr);
-        const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+        const Moments<R> m = node_moments(a, fr, gr, n);
         const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
         acc[0] += uy * phi;
         acc[1] += ux * ux + uy * uy + uz * uz;
@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kObsThreads) profile_kernel(const StepArgs<S> 
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
         gather<S, SWAPPED>(a, g, fr, gr);
-        const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+        const Moments<R> m = node_moments(a, fr, gr, n);
         acc[0] += (double)m.ux;
         acc[1] += (double)m.uy;
         acc[2] += (double)m.uz;
@@ -206,12 +206,11 @@ __global__ void export_pop_kernel(const StepArgs<S> a, int which, int k, double 
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.nodes) return;
     const Node g = make_node<PERIODIC>(a, n);
-    const S *base = which ? a.g : a.f;
     double v = 0.0;
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if (K == k) {
-            const S s = load_pop<S, SWAPPED, K>(base, a.ps, g);
+            const S s = load_pop<S, SWAPPED, K>(which ? a.gl : a.fl, g);
             v = which ? (double)C::template g_in<K>(s, a.t0) : (double)C::template f_in<K>(s, a.t0);
         }
     });
@@ -227,7 +226,7 @@ __global__ void export_macro_kernel(const StepArgs<S> a, double *__restrict__ ou
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     gather<S, SWAPPED>(a, g, fr, gr);
-    const Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+    const Moments<R> m = node_moments(a, fr, gr, n);
     const size_t N = a.nodes;
     out[n] = (double)m.rho;
     out[N + n] = (double)m.ux;
@@ -242,13 +241,15 @@ __global__ void import_pop_kernel(const StepArgs<S> a, int which, int k, const d
     using C = Codec<S>;
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.nodes) return;
-    S *base = which ? a.g : a.f;
     const double v = in[n];
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if (K == k) {
             using R = typename C::R;
-            base[(int64_t)K * a.ps + n] = which ? C::template g_out<K>((R)v, a.t0) : C::template f_out<K>((R)v, a.t0);
+            if (which)
+                a.gs[K][n] = C::template g_out<K>((R)v, a.t0);
+            else
+                a.fs[K][n] = C::template f_out<K>((R)v, a.t0);
         }
     });
 }
@@ -291,10 +292,26 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         const double gk = __dmul_rn(wd(K), t);
-        a.f[(int64_t)K * a.ps + n] = C::template f_out<K>((R)0, a.t0);
-        a.g[(int64_t)K * a.ps + n] = C::template g_out<K>((R)gk, a.t0);
+        a.fs[K][n] = C::template f_out<K>((R)0, a.t0);
+        a.gs[K][n] = C::template g_out<K>((R)gk, a.t0);
     });
     a.phip[n] = (typename C::P)t;
+}
+
+// Counts dividends a for which div_by(a, b, RN(1/b)) differs from the
+// hardware's correctly rounded a / b: random signs, 52-bit mantissas and
+// exponents in [-60, 10].
+__global__ void division_check_kernel(double b, double y, uint64_t n, uint64_t key, unsigned long long *bad) {
+    unsigned long long cnt = 0;
+    for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x) {
+        const uint64_t r = splitmix64(key + i);
+        const double m = 1.0 + (double)(r >> 12) * (1.0 / 4503599627370496.0);
+        const int e = (int)((r & 0x7f) % 71) - 60;
+        double a = scalbn(m, e);
+        if ((r >> 7) & 1) a = -a;
+        if (div_by(a, b, y) != __ddiv_rn(a, b)) cnt++;
+    }
+    if (cnt) atomicAdd(bad, cnt);
 }
 
 }  // namespace lbm
@@ -309,6 +326,7 @@ struct lbm_case {
     int64_t step = 0;
     bool swapped = false;
     bool initialised = false;
+    bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
     void *f = nullptr, *g = nullptr, *phip = nullptr;
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
@@ -349,18 +367,22 @@ int obs_blocks_for(int64_t nodes) {
 template <class S> StepArgs<S> make_args(const lbm_case *c) {
     using R = typename Codec<S>::R;
     StepArgs<S> a;
-    a.f = (S *)c->f;
-    a.g = (S *)c->g;
-    a.f_st = (S *)c->f;
-    a.g_st = (S *)c->g;
+    for (int k = 0; k < Q; k++) {
+        a.fl[k] = a.fs[k] = (S *)c->f + (size_t)k * (size_t)c->ps;
+        a.gl[k] = a.gs[k] = (S *)c->g + (size_t)k * (size_t)c->ps;
+    }
     a.phip = (typename Codec<S>::P *)c->phip;
-    a.ps = c->ps;
     a.lx = c->p.lx;
     a.ly = c->p.ly;
     a.lz = c->p.lz;
     a.nodes = (uint32_t)c->nodes;
     a.div_lx = FastDiv((uint32_t)c->p.lx);
     a.div_ly = FastDiv((uint32_t)c->p.ly);
+    a.tau = (R)c->d.tau;
+    a.tauc = (R)c->d.tauc;
+    a.rcp_tau = (R)(1.0 / c->d.tau);
+    a.rcp_tauc = (R)(1.0 / c->d.tauc);
+    a.rcp_rt = (R)(1.0 / (1.0 / 3.0));
     a.omega_f = (R)(1.0 / c->d.tau);
     a.omega_g = (R)(1.0 / c->d.tauc);
     a.force_fac = (R)(1.0 - 0.5 / c->d.tau);
@@ -368,6 +390,8 @@ template <class S> StepArgs<S> make_args(const lbm_case *c) {
     a.t0 = (R)c->d.t0;
     a.t_hot = (R)c->p.t_hot;
     a.t_cold = (R)c->p.t_cold;
+    a.use_phi_fix = c->rest_phi ? 1 : 0;
+    a.phi_fix = (R)0.5;
     return a;
 }
 
@@ -527,6 +551,7 @@ static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, v
     c->swapped = false;
     c->step = 0;
     c->initialised = true;
+    c->rest_phi = mode == 0;
     return LBM_OK;
 }
 
@@ -544,16 +569,31 @@ int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const d
     if (!uy || !f || !g) return fail(LBM_ERR_ARG, "uy, f and g are required");
     DeviceGuard dg(c->p.device);
     const int64_t N = c->nodes;
-    // previous-step temperature from uy = sum(c_y f) + g*beta*(phi_prev - t0)/2
+    // Previous-step temperature from uy = sum(c_y f) + g*beta*(phi_prev - t0)/2.
+    // For FP64 storage the estimate is nudged, one ulp at a time, until the
+    // device's own formula, jy + 0.5*(gb*(phi_prev - t0)), gives back the
+    // file's uy bit for bit, so the first step uses the velocity the
+    // reference would use.
     std::vector<double> pp((size_t)N);
     const double gb = c->p.gravity * c->p.beta;
+    const double t0 = c->d.t0;
+    const bool exact = c->p.storage == LBM_STORE_F64;
     for (int64_t i = 0; i < N; i++) {
         double jy = 0.0;
         for (int k = 0; k < Q; k++) {
             if (cy(k) > 0) jy += f[(size_t)k * N + i];
             if (cy(k) < 0) jy -= f[(size_t)k * N + i];
         }
-        pp[(size_t)i] = c->d.t0 + 2.0 * (uy[i] - jy) / gb;
+        double p = t0 + 2.0 * (uy[i] - jy) / gb;
+        if (exact && std::isfinite(p)) {
+            for (int it = 0; it < 64; it++) {
+                const volatile double h = gb * (p - t0);
+                const volatile double u = jy + 0.5 * h;
+                if (u == uy[i]) break;
+                p = std::nextafter(p, u < uy[i] ? INFINITY : -INFINITY);
+            }
+        }
+        pp[(size_t)i] = p;
     }
     double *stage = nullptr;
     CUDA_TRY(cudaMalloc(&stage, (size_t)N * sizeof(double)));
@@ -579,6 +619,7 @@ int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const d
     c->swapped = false;
     c->step = 0;
     c->initialised = true;
+    c->rest_phi = false;
     return LBM_OK;
 }
 
@@ -632,10 +673,12 @@ int lbm_step(lbm_case *c, int32_t nsteps, void *stream) {
     cudaStream_t st = (cudaStream_t)stream;
     rc = with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
-        const StepArgs<S> a = make_args<S>(c);
+        StepArgs<S> a = make_args<S>(c);
         for (int s = 0; s < nsteps; s++) {
             launch_step<S>(c, a, st);
             c->swapped = !c->swapped;
+            c->rest_phi = false;
+            a.use_phi_fix = 0;
         }
         return LBM_OK;
     });
@@ -704,7 +747,7 @@ struct CheckpointHeader {
     lbm_params p;
     int64_t step;
     int32_t swapped;
-    int32_t reserved;
+    int32_t flags;          // bit 0: next step uses the rest state's phi = 0.5
     int64_t ps;
 };
 
@@ -739,6 +782,7 @@ int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
     h.p = c->p;
     h.step = c->step;
     h.swapped = c->swapped ? 1 : 0;
+    h.flags = c->rest_phi ? 1 : 0;
     h.ps = c->ps;
     std::memcpy(host, &h, sizeof h);
     cudaStream_t st = (cudaStream_t)stream;
@@ -770,7 +814,26 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
     CUDA_TRY(cudaMemcpyAsync(c->phip, b + op, cb, cudaMemcpyHostToDevice, st));
     c->step = h.step;
     c->swapped = h.swapped != 0;
+    c->rest_phi = (h.flags & 1) != 0;
     c->initialised = true;
+    return LBM_OK;
+}
+
+int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed, uint64_t *mismatches) {
+    if (!mismatches || !(divisor > 0) || !std::isfinite(divisor)) return fail(LBM_ERR_ARG, "bad arguments");
+    DeviceGuard dg(device);
+    unsigned long long *d = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(unsigned long long)));
+    cudaError_t e = cudaMemset(d, 0, sizeof(unsigned long long));
+    if (e == cudaSuccess) {
+        division_check_kernel<<<148 * 8, 256>>>(divisor, 1.0 / divisor, n, seed, d);
+        e = cudaGetLastError();
+    }
+    unsigned long long h = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof h, cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    *mismatches = h;
     return LBM_OK;
 }
 

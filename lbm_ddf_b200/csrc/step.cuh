@@ -44,24 +44,35 @@ namespace lbm {
 template <class S> struct StepArgs {
     using R = typename Codec<S>::R;
     using P = typename Codec<S>::P;
-    S *f;              // 27 populations, population k at f + k*ps
-    S *g;
-    // The same two arrays again, used only for the stores.  In the
+    // Base address of each population row (row k of f at fl[k]).  Kernel
+    // parameters live in the constant bank, so an access costs one
+    // multiply-add of a 32-bit node index onto a constant, whatever the
+    // case's size.
+    S *fl[Q];
+    S *gl[Q];
+    // The same addresses again, used only for the stores.  In the
     // natural-layout step every store address equals a load address; forming
-    // it from a separate base keeps the compiler from holding all 54 load
+    // it from separate bases keeps the compiler from holding all 54 load
     // addresses live across the collision (which costs ~110 registers).
-    S *f_st;
-    S *g_st;
+    S *fs[Q];
+    S *gs[Q];
     P *phip;           // previous-step temperature, one per node
-    int64_t ps;        // population stride in elements (>= nodes)
     int32_t lx, ly, lz;
     uint32_t nodes;
     FastDiv div_lx, div_ly;
+    R tau, tauc;       // relaxation times (the FP64 path divides by them)
+    R rcp_tau, rcp_tauc, rcp_rt;   // their correctly rounded reciprocals, and that of 1/3
     R omega_f;         // 1/tau
     R omega_g;         // 1/tauc
     R force_fac;       // 1 - 1/(2 tau)
     R gb;              // gravity*beta
     R t0, t_hot, t_cold;
+    // The reference's rest state (src/initial.cu:218-240) stores phi = 0.5
+    // while its populations w_i * 0.5 sum to 0.5 - 2^-54; its first step
+    // collides with the stored 0.5.  When set, the moments use phi_fix
+    // instead of sum(g) (one step after lbm_init_rest).
+    int32_t use_phi_fix;
+    R phi_fix;
 };
 
 // Geometry of one node: coordinates, and node-index displacements to the
@@ -118,13 +129,14 @@ __device__ __forceinline__ bool inside(const Node &g) {
            (DZ < 0 ? g.vzm : DZ > 0 ? g.vzp : true);
 }
 
-// Population k of node g at the current time, from either layout.
+// Population k of node g at the current time, from either layout; rows[k]
+// is the base of population row k.
 template <class S, bool SWAPPED, int K>
-__device__ __forceinline__ S load_pop(const S *__restrict__ base, int64_t ps, const Node &g) {
-    if (!SWAPPED) return base[(int64_t)K * ps + g.n];
+__device__ __forceinline__ S load_pop(S *const (&rows)[Q], const Node &g) {
+    if (!SWAPPED) return rows[K][g.n];
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
-    if (inside<DX, DY, DZ>(g)) return base[(int64_t)opp(K) * ps + (int64_t)((int64_t)g.n + disp<DX, DY, DZ>(g))];
-    return base[(int64_t)K * ps + g.n];
+    if (inside<DX, DY, DZ>(g)) return rows[opp(K)][(int32_t)g.n + disp<DX, DY, DZ>(g)];
+    return rows[K][g.n];
 }
 
 template <class S, bool SWAPPED>
@@ -133,8 +145,8 @@ __device__ __forceinline__ void gather(const StepArgs<S> &a, const Node &g, type
     using C = Codec<S>;
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K>(a.f, a.ps, g), a.t0);
-        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K>(a.g, a.ps, g), a.t0);
+        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K>(a.fl, g), a.t0);
+        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K>(a.gl, g), a.t0);
     });
 }
 
@@ -167,10 +179,23 @@ __device__ __forceinline__ Moments<R> moments(const R (&fr)[Q], const R (&gr)[Q]
     return m;
 }
 
-// BGK collision of f (with the buoyancy force) and g, in place on fr/gr.
+template <class S>
+__device__ __forceinline__ Moments<typename Codec<S>::R> node_moments(const StepArgs<S> &a,
+                                                                     const typename Codec<S>::R (&fr)[Q],
+                                                                     const typename Codec<S>::R (&gr)[Q],
+                                                                     uint32_t n) {
+    using R = typename Codec<S>::R;
+    Moments<R> m = moments(fr, gr, (R)a.phip[n], a.gb, a.t0);
+    if (a.use_phi_fix) m.phi = a.phi_fix;
+    return m;
+}
+
+// BGK collision of f (with the buoyancy force) and g, in place on fr/gr,
+// in FP32: the same equilibria with the divisions by 1/3 and tau folded into
+// multiplications and every multiply-add left to the compiler.
 template <class R>
-__device__ __forceinline__ void collide(R (&fr)[Q], R (&gr)[Q], const Moments<R> &m, R omega_f, R omega_g,
-                                        R force_fac, R gb, R t0) {
+__device__ __forceinline__ void collide_fast(R (&fr)[Q], R (&gr)[Q], const Moments<R> &m, R omega_f, R omega_g,
+                                             R force_fac, R gb, R t0) {
     const R uv = R(3) * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
     const R fy = gb * (m.phi - t0);           // force of this step, from phi^{n-1}
     const R kf = R(3) * force_fac * fy;
@@ -195,6 +220,84 @@ __device__ __forceinline__ void collide(R (&fr)[Q], R (&gr)[Q], const Moments<R>
     });
 }
 
+// Correctly rounded a / b for a divisor b known in advance, from its correctly
+// rounded reciprocal y = RN(1/b): q = RN(a y), r = a - b q (exact by FMA),
+// result RN(q + r y).  Markstein's theorem (P. Markstein, IBM J. Res. Dev.
+// 34(1), 1990; "IA-64 and Elementary Functions", 2000, Thm 8.10): if y is
+// within half an ulp of 1/b and q within one ulp of a/b, the corrected
+// quotient is the correctly rounded one.  Valid for finite quotients away
+// from the subnormal range (all quotients here); the C ABI's
+// lbm_selfcheck_division checks it against the hardware division on the GPU.
+__device__ __forceinline__ double div_by(double a, double b, double y) {
+    const double q = __dmul_rn(a, y);
+    const double r = __fma_rn(-b, q, a);
+    return __fma_rn(r, y, q);
+}
+
+// The same collision in FP64 as the reference binary computes it: the
+// operations of src/collision.cu:19-33 and :65-72 in their order, correctly
+// rounded divisions by RT = 1/3, tau and tauc, and a fused multiply-add
+// exactly where the reference build has one (u*u sums, eu*eu - uv, f - w*feq,
+// g - w*phi*geq; not the force term).  Written with round-to-nearest
+// intrinsics, which the compiler never re-fuses, so the results are bitwise
+// the reference's.
+__device__ __forceinline__ void collide_exact(double (&fr)[Q], double (&gr)[Q], const Moments<double> &m,
+                                              double tau, double tauc, double rcp_tau, double rcp_tauc,
+                                              double rcp_rt, double force_fac, double gb, double t0) {
+    const double RT = 1.0 / 3.0;
+    const double uv = div_by(__fma_rn(m.uz, m.uz, __fma_rn(m.ux, m.ux, __dmul_rn(m.uy, m.uy))), RT, rcp_rt);
+    const double fy = __dmul_rn(gb, __dsub_rn(m.phi, t0));
+    const double kf = __dmul_rn(force_fac, fy);
+    // ((1 - 1/(2 tau)) F_y (c_y - u_y)) / RT takes one of three values
+    const double fc_m = div_by(__dmul_rn(kf, __dsub_rn(-1.0, m.uy)), RT, rcp_rt);
+    const double fc_0 = div_by(__dmul_rn(kf, __dsub_rn(0.0, m.uy)), RT, rcp_rt);
+    const double fc_p = div_by(__dmul_rn(kf, __dsub_rn(1.0, m.uy)), RT, rcp_rt);
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        constexpr double w = wd(K);
+        double cu = 0.0;   // (c.u), summed x, y, z as the reference does; c*u is exact
+        if (cx(K) > 0) cu = __dadd_rn(cu, m.ux);
+        if (cx(K) < 0) cu = __dsub_rn(cu, m.ux);
+        if (cy(K) > 0) cu = __dadd_rn(cu, m.uy);
+        if (cy(K) < 0) cu = __dsub_rn(cu, m.uy);
+        if (cz(K) > 0) cu = __dadd_rn(cu, m.uz);
+        if (cz(K) < 0) cu = __dsub_rn(cu, m.uz);
+        const double eu = div_by(cu, RT, rcp_rt);
+        const double hq = __dmul_rn(0.5, __fma_rn(eu, eu, -uv));
+        const double feq_in = __dadd_rn(__dadd_rn(m.rho, eu), hq);
+        const double inner0 = __dadd_rn(__dadd_rn(1.0, eu), hq);
+        const double feq0 = __dmul_rn(w, inner0);
+        const double fc = cy(K) < 0 ? fc_m : cy(K) > 0 ? fc_p : fc_0;
+        const double fo = fr[K];
+        double fch = -div_by(__fma_rn(-w, feq_in, fo), tau, rcp_tau);
+        fch = __dadd_rn(fch, __dmul_rn(fc, feq0));
+        fr[K] = __dadd_rn(fo, fch);
+        const double go = gr[K];
+        const double gch = -div_by(__fma_rn(-__dmul_rn(w, m.phi), inner0, go), tauc, rcp_tauc);
+        gr[K] = __dadd_rn(go, gch);
+    });
+}
+
+template <class S>
+__device__ __forceinline__ void collide(typename Codec<S>::R (&fr)[Q], typename Codec<S>::R (&gr)[Q],
+                                        const Moments<typename Codec<S>::R> &m, const StepArgs<S> &a) {
+    if constexpr (std::is_same<typename Codec<S>::R, double>::value)
+        collide_exact(fr, gr, m, a.tau, a.tauc, a.rcp_tau, a.rcp_tauc, a.rcp_rt, a.force_fac, a.gb, a.t0);
+    else
+        collide_fast(fr, gr, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+}
+
+// Anti-bounce-back value of an outgoing population gv at a plate of
+// temperature tw: -gv + 2 w tw (1 + rho), src/streaming.cu:207-227 (the
+// product fused into the sum in FP64, as the reference build does).
+template <int I, class R>
+__device__ __forceinline__ R abb(R gv, R tw, R rho) {
+    if constexpr (std::is_same<R, double>::value)
+        return __fma_rn(__dmul_rn(__dmul_rn(2.0, wd(I)), tw), __dadd_rn(1.0, rho), -gv);
+    else
+        return -gv + R(2) * R(wd(I)) * tw * (R(1) + rho);
+}
+
 // Write the post-collision populations of node g to where the next step
 // reads them.  rho is the node's pre-collision density (for anti-bounce-back).
 template <class S, bool SWAPPED, bool PERIODIC>
@@ -202,8 +305,6 @@ __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, con
                                         const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
     using C = Codec<S>;
     using R = typename C::R;
-    const R abb_hot = R(2) * a.t_hot * (R(1) + rho);
-    const R abb_cold = R(2) * a.t_cold * (R(1) + rho);
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
@@ -211,24 +312,22 @@ __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, con
         R gv = gr[I];
         const bool out_y = (DY < 0 && !g.vym) || (DY > 0 && !g.vyp);
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
-        if (DY != 0 && out_y && !out_z) gv = -gv + R(wd(I)) * (DY < 0 ? abb_hot : abb_cold);
-        int64_t off;
-        if (!SWAPPED) {
-            off = (int64_t)opp(I) * a.ps + g.n;
-        } else if (inside<DX, DY, DZ>(g)) {
-            off = (int64_t)I * a.ps + (int64_t)((int64_t)g.n + disp<DX, DY, DZ>(g));
+        if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
+        if (SWAPPED && inside<DX, DY, DZ>(g)) {
+            const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
+            a.fs[I][j] = C::template f_out<I>(fv, a.t0);
+            a.gs[I][j] = C::template g_out<I>(gv, a.t0);
         } else {
-            off = (int64_t)opp(I) * a.ps + g.n;
+            a.fs[opp(I)][g.n] = C::template f_out<I>(fv, a.t0);
+            a.gs[opp(I)][g.n] = C::template g_out<I>(gv, a.t0);
         }
-        a.f_st[off] = C::template f_out<I>(fv, a.t0);
-        a.g_st[off] = C::template g_out<I>(gv, a.t0);
     });
 }
 
-// Resident blocks per SM the register allocation is sized for: 3 x 128
-// threads (<= 168 registers) for 4-byte and 2-byte storage, 2 (<= 255) for
+// Resident blocks per SM the register allocation is sized for: 4 x 128
+// threads (<= 128 registers) for 4-byte and 2-byte storage, 2 (<= 255) for
 // FP64, which holds 54 doubles across the collision.
-template <class S> struct StepOccupancy { static constexpr int value = sizeof(S) == 8 ? 2 : 3; };
+template <class S> struct StepOccupancy { static constexpr int value = sizeof(S) == 8 ? 2 : 4; };
 
 template <class S, bool SWAPPED, bool PERIODIC>
 __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
@@ -238,9 +337,8 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     gather<S, SWAPPED>(a, g, fr, gr);
-    const R pp = (R)a.phip[n];
-    const Moments<R> m = moments(fr, gr, pp, a.gb, a.t0);
-    collide(fr, gr, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+    const Moments<R> m = node_moments(a, fr, gr, n);
+    collide<S>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
     scatter<S, SWAPPED, PERIODIC>(a, g, fr, gr, m.rho);
 }

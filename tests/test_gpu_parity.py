@@ -2,7 +2,10 @@
 and with the CPU oracle.
 
 Tolerances (field-relative, max|a-b| / max|b|):
-  FP64 storage      populations 1e-12, macroscopic fields 1e-12, Nu 1e-10
+  FP64 storage      bitwise equal populations and macroscopic fields (the
+                    FP64 path rounds exactly as the reference binary does);
+                    the north-star bounds 1e-12 (fields) and 1e-10 (Nu) are
+                    asserted as well; Nu from the device reduction 1e-10
   FP32 storage      5e-5 after <= 200 steps (FP32 arithmetic)
   FP16S / BF16S     5e-3 / 4e-2 after <= 100 steps (16-bit storage)
 """
@@ -54,10 +57,13 @@ def oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=None, amplitude=1e-
     return o
 
 
-def compare(got, o, tol, fields=FIELDS):
+def compare(got, o, tol, fields=FIELDS, bitwise=False):
     for k in fields:
         e = relerr(got[k].reshape(-1), o.field(k).reshape(-1))
         assert e <= tol, f"{k}: {e:.3e} > {tol:.1e}"
+        if bitwise:
+            diff = int(np.sum(got[k].reshape(-1) != o.field(k).reshape(-1)))
+            assert diff == 0, f"{k}: {diff} values differ from the oracle"
 
 
 # ---------------------------------------------------------------- reference
@@ -89,8 +95,10 @@ def test_f64_matches_reference_outputs(lbm, oracle_mod, name):
         if "sample_nodes" in g:
             a = a[:, g["sample_nodes"]]
         assert relerr(a.reshape(-1), g[k].reshape(-1)) <= 1e-12, k
+        assert np.array_equal(a.reshape(-1), g[k].reshape(-1)), k + " not bitwise the reference's"
     for k in ("rho", "ux", "uy", "uz", "phi"):
         assert relerr(got[k].reshape(-1), g[k]) <= 1e-12, k
+        assert np.array_equal(got[k].reshape(-1), g[k]), k + " not bitwise the reference's"
     d = lbm.derive(p)
     ref_nu = nu_from_fields(g["uy"], g["phi"], c["lx"], c["ly"], c["lz"], d["diff"])
     eng = (got["obs"]["nu_bulk"], got["obs"]["nu_top"], got["obs"]["nu_bottom"])
@@ -99,6 +107,18 @@ def test_f64_matches_reference_outputs(lbm, oracle_mod, name):
 
 
 # ---------------------------------------------------------------- oracle, FP64
+
+def test_fp64_division_identity(lbm):
+    """The FP64 collision divides by 1/3, tau and tauc through their
+    reciprocals with one Markstein correction; that must be the correctly
+    rounded quotient, as the reference's divisions are."""
+    divisors = [1.0 / 3.0]
+    for ly, ra, pr in [(64, 1e5, 0.71), (256, 1e7, 0.71), (256, 1e8, 0.71), (48, 1e8, 7.0), (10, 1e5, 0.71)]:
+        d = lbm.derive(lbm.make_params(ly, ly, ly, rayleigh=ra, prandtl=pr))
+        divisors += [d["tau"], d["tauc"]]
+    for b in divisors:
+        assert lbm.selfcheck_division(b, n=1 << 25, seed=7) == 0, b
+
 
 def test_f64_init_is_bitwise_the_oracles(lbm, oracle_mod):
     lx, ly, lz = 20, 14, 9
@@ -117,13 +137,17 @@ def test_f64_matches_oracle(lbm, oracle_mod, periodic, steps):
     p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
     got = engine_run(lbm, p, steps, seed=5)
     o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=5)
-    compare(got, o, 1e-12)
+    compare(got, o, 1e-12, bitwise=True)
     ob = o.observables()
     for k in ("nu_bulk", "nu_top", "nu_bottom", "ke", "re", "phi_mean"):
         assert abs(got["obs"][k] - ob[k]) <= 1e-10 * max(1.0, abs(ob[k])), k
     for k in ("ux_mean", "uy_mean", "uz_mean"):
         assert abs(got["obs"][k] - ob[k]) <= 1e-14, k
-    np.testing.assert_allclose(got["profile"], o.profile(), rtol=1e-11, atol=1e-15)
+    pa, pb = got["profile"], o.profile()
+    np.testing.assert_allclose(pa[:, :4], pb[:, :4], rtol=1e-11, atol=1e-15)
+    # phi_rms is a one-pass variance, sqrt(<phi^2> - <phi>^2) (src/output.cu:358):
+    # its square is a difference of two O(1) sums, good to ~1e-15 absolute
+    np.testing.assert_allclose(pa[:, 4] ** 2, pb[:, 4] ** 2, rtol=0, atol=1e-13)
 
 
 def test_f64_step_chunking_is_irrelevant(lbm):
@@ -141,7 +165,7 @@ def test_f64_larger_box_vs_oracle(lbm, oracle_mod):
         p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
         got = engine_run(lbm, p, steps, seed=11)
         o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=11)
-        compare(got, o, 1e-12)
+        compare(got, o, 1e-12, bitwise=True)
 
 
 def test_load_store_roundtrip(lbm, oracle_mod):
@@ -155,7 +179,11 @@ def test_load_store_roundtrip(lbm, oracle_mod):
 
 
 def test_xz_mirror_symmetry(lbm):
-    """A state symmetric under x <-> z stays symmetric (D3Q27 is)."""
+    """A state symmetric under x <-> z stays symmetric (D3Q27 is), with
+    periodic sides.  In the closed box the reference's own wall precedence
+    is not x/z symmetric (on x/y edges the plate rule wins, on y/z edges the
+    side-wall rule wins, src/streaming.cu:183-250), so the symmetry is
+    checked where it holds."""
     from oracle.oracle import CX, CY, CZ, W
 
     lx = lz = 12
@@ -168,7 +196,7 @@ def test_xz_mirror_symmetry(lbm):
     t = t + noise
     g = W[:, None, None, None] * t[None]
     f = np.zeros_like(g)
-    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_WALL, storage="f64")
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage="f64")
     uy = 0.5 * p.gravity * p.beta * (t - 0.5)
     st = dict(rho=np.zeros(n), ux=np.zeros(n), uy=uy, uz=np.zeros(n), phi=t, f=f, g=g)
     got = engine_run(lbm, p, 40, state=st)
@@ -195,11 +223,14 @@ def test_mass_is_conserved(lbm):
 @pytest.mark.parametrize("storage,tol,steps", [("f32", 5e-5, 200), ("f16s", 5e-3, 100), ("bf16s", 4e-2, 100)])
 @pytest.mark.parametrize("periodic", [True, False])
 def test_reduced_precision_vs_oracle(lbm, oracle_mod, storage, tol, steps, periodic):
+    """Populations and temperature within tol; the velocity, a sum of
+    populations that cancel to ~1e-3 of their size, within 20 tol."""
     lx, ly, lz = 24, 20, 16
     p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage=storage)
     got = engine_run(lbm, p, steps, seed=21, amplitude=1e-2)
     o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=21, amplitude=1e-2)
-    compare(got, o, tol, fields=("f", "g", "phi", "uy"))
+    compare(got, o, tol, fields=("f", "g", "phi"))
+    compare(got, o, 20 * tol, fields=("uy",))
     ob = o.observables()
     assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= 50 * tol
 
