@@ -160,6 +160,34 @@ int lbm_checkpoint_bytes(const lbm_case *c, uint64_t *bytes);
 int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream);
 int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *stream);
 
+/* Observables without allocating: the lbm_get_observables reduction over
+ * populations the caller holds in memory of its own, for callers that may
+ * not allocate device memory through this library (while a stream is being
+ * captured, under a fixed HBM budget, or on a thread that must not block on
+ * cudaMalloc / cudaFree).  No counterpart in the reference.
+ *   f, g      27 population rows each, row k at base + k*pop_stride elements,
+ *             in p->storage's format and in the layout `swapped` names
+ *             (0 natural, 1 swapped; a case's layout is swapped after an odd
+ *             number of steps from an init or load);
+ *   phi_prev  previous-step temperature per node (double for F64, else float);
+ *   out_dev   DEVICE memory for one lbm_observables, written on `stream`.
+ * Enqueues two kernels on `stream` and returns without synchronising; the
+ * caller reads out_dev after the stream.  The block partial sums go to a
+ * fixed array inside the library (1184 rows of 13 doubles, 123 KB, held by
+ * every GPU that loads the library until the process exits); it covers any
+ * grid the C ABI accepts (fewer than 2^31 nodes) and calls needing more rows
+ * are rejected with LBM_ERR_ARG.  Each call overwrites every row it reads,
+ * so nothing has to be cleared between calls, but calls whose kernels
+ * overlap on the GPU (other streams, other host threads) race on the array.
+ * The first call on a device looks up the array's address; make that first
+ * call before any stream capture.  It knows nothing of a case's history, so
+ * for the state right after lbm_init_rest (step 0) it reports the mean
+ * temperature from sum(g) = 0.5 - 2^-54 where lbm_get_observables reports
+ * the rest state's stored 0.5. */
+int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, const void *phi_prev,
+                            uint64_t pop_stride, int32_t swapped, int64_t step,
+                            lbm_observables *out_dev, void *stream);
+
 /* Device self-check of the division identity the FP64 path uses for its
  * constant divisors (a / b from the correctly rounded reciprocal with one
  * Markstein correction): counts, over n random dividends, the results that

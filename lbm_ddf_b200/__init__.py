@@ -99,11 +99,13 @@ def lib() -> C.CDLL:
         L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
         L.lbm_save_state.argtypes = [vp, vp, C.c_uint64, vp]
         L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
+        L.lbm_observables_noalloc.argtypes = [P, vp, vp, vp, C.c_uint64, C.c_int32, C.c_int64, vp, vp]
         L.lbm_selfcheck_division.argtypes = [C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
         for name in ("lbm_derive", "lbm_case_bytes", "lbm_create", "lbm_destroy", "lbm_init_rest",
                      "lbm_init_conduction", "lbm_load_ref_state", "lbm_store_ref_state", "lbm_step",
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
-                     "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division"):
+                     "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
+                     "lbm_observables_noalloc"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -194,6 +196,18 @@ def selfcheck_division(divisor: float, n: int = 1 << 24, seed: int = 1, device: 
     bad = C.c_uint64()
     check(lib().lbm_selfcheck_division(device, divisor, n, seed, C.byref(bad)))
     return int(bad.value)
+
+
+def observables_noalloc(params: LbmParams, f_ptr: int, g_ptr: int, phi_prev_ptr: int, pop_stride: int,
+                        swapped: bool, step: int, out_dev_ptr: int, stream=None) -> None:
+    """Enqueue the observables reduction over caller-owned device buffers
+    into the lbm_observables at device address out_dev_ptr, allocating
+    nothing (the C ABI's lbm_observables_noalloc: for callers that must not
+    allocate device memory, e.g. while capturing a CUDA graph).  Returns
+    without synchronising."""
+    check(lib().lbm_observables_noalloc(C.byref(params), C.c_void_p(f_ptr), C.c_void_p(g_ptr),
+                                        C.c_void_p(phi_prev_ptr), pop_stride, int(bool(swapped)), int(step),
+                                        C.c_void_p(out_dev_ptr), _stream_handle(stream)))
 
 
 def case_bytes(p: LbmParams) -> int:

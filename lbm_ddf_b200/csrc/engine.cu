@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <string>
 #include <vector>
@@ -816,6 +817,93 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
     c->swapped = h.swapped != 0;
     c->rest_phi = (h.flags & 1) != 0;
     c->initialised = true;
+    return LBM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Observables without allocating.
+//
+// For callers that hold their populations in memory they manage themselves
+// and may not allocate device memory from this library: code that runs while
+// a CUDA stream is being captured into a graph, a serving loop whose whole
+// HBM budget is accounted for up front, or a host thread that must not block
+// (cudaMalloc and cudaFree synchronise the device).  The reduction's block
+// partial sums live in this fixed device array instead of an allocation; the
+// array is part of the library image, so every GPU that loads the library
+// holds it (kNoAllocRows x 13 doubles = 123 KB) until the process exits.
+// ---------------------------------------------------------------------------
+constexpr int kNoAllocRows = 148 * 8;   // most reduction blocks one call runs
+static __device__ __align__(256) double g_noalloc_partials[kNoAllocRows * kObs];
+
+namespace {
+std::mutex g_noalloc_mu;
+void *g_noalloc_ptr[256];               // device address of the array, per device ordinal
+
+// Looks up the array's device address once per device, with that device
+// current; host code cannot use the symbol itself as a device address.
+int noalloc_scratch(int device, double **out) {
+    if (device < 0 || device >= 256) return fail(LBM_ERR_ARG, "device ordinal out of range");
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[device]) {
+        void *ptr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&ptr, g_noalloc_partials);
+        if (e != cudaSuccess || !ptr)
+            return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_partials): ") +
+                                          cudaGetErrorString(e));
+        g_noalloc_ptr[device] = ptr;
+    }
+    *out = (double *)g_noalloc_ptr[device];
+    return LBM_OK;
+}
+}  // namespace
+
+int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, const void *phi_prev,
+                            uint64_t pop_stride, int32_t swapped, int64_t step, lbm_observables *out_dev,
+                            void *stream) {
+    int rc = check_params(p);
+    if (rc) return rc;
+    if (!f || !g || !phi_prev || !out_dev) return fail(LBM_ERR_ARG, "f, g, phi_prev and out_dev are required");
+    const int64_t nodes = (int64_t)p->lx * p->ly * p->lz;
+    if ((int64_t)pop_stride < nodes) return fail(LBM_ERR_ARG, "pop_stride is smaller than the node count");
+    if (pop_stride > (1ull << 40)) return fail(LBM_ERR_ARG, "pop_stride too large");
+    const int blocks = obs_blocks_for(nodes);
+    if (blocks > kNoAllocRows)
+        return fail(LBM_ERR_ARG, "reduction needs more partial rows than the fixed scratch holds");
+    DeviceGuard dg(p->device);
+    double *scratch = nullptr;
+    rc = noalloc_scratch(p->device, &scratch);
+    if (rc) return rc;
+    lbm_case view;               // a stack view of the caller's buffers; owns nothing
+    view.p = *p;
+    derive(p, &view.d);
+    view.nodes = nodes;
+    view.ps = (int64_t)pop_stride;
+    view.step = step;
+    view.swapped = swapped != 0;
+    view.initialised = true;
+    view.f = const_cast<void *>(f);
+    view.g = const_cast<void *>(g);
+    view.phip = const_cast<void *>(phi_prev);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = with_storage(&view, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const StepArgs<S> a = make_args<S>(&view);
+        const lbm_case *c = &view;
+        LBM_DISPATCH_LAYOUT(c, obs_kernel, blocks, kObsThreads, st, a, scratch);
+        ObsConsts k;
+        k.nodes = (double)nodes;
+        k.plane = (double)p->lx * (double)p->lz;
+        k.ly = (double)p->ly;
+        k.diff = view.d.diff;
+        k.dT = p->t_hot - p->t_cold;
+        k.visc = view.d.visc;
+        k.step = step;
+        obs_finalize<<<1, 32, 0, st>>>(scratch, blocks, k, out_dev);
+        return LBM_OK;
+    });
+    view.f = view.g = view.phip = nullptr;
+    if (rc) return rc;
+    CUDA_TRY(cudaGetLastError());
     return LBM_OK;
 }
 
