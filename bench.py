@@ -195,7 +195,10 @@ def run_engine(args):
     stream = torch.cuda.Stream(device=dev)
     bytes_per_lu = 2 * 27 * 2 * lbm.STORAGE_BYTES[p.storage]
 
+    kind = {"auto": lbm.KERNEL_AUTO, "node": lbm.KERNEL_NODE, "row": lbm.KERNEL_ROW}[args.kernel]
     case = lbm.Case(p)
+    case.set_step_kernel(kind)
+    kernel_used = {lbm.KERNEL_NODE: "node", lbm.KERNEL_ROW: "row"}[case.step_kernel]
     case.init_conduction(1000 + rank, 1e-3, stream=stream)
     case.step(args.warmup, stream=stream)
     torch.cuda.synchronize()
@@ -215,6 +218,7 @@ def run_engine(args):
     case.save_state(host, stream=stream)
     torch.cuda.synchronize()
     e2e_case = lbm.Case(p)
+    e2e_case.set_step_kernel(kind)
     barrier(world)
     t0 = time.perf_counter()
     e2e_case.restore_state(host, stream=stream)
@@ -237,6 +241,7 @@ def run_engine(args):
         p64 = lbm.make_params(w["lx"], w["ly"], w["lz"], rayleigh=w["rayleigh"], prandtl=w["prandtl"],
                               sides=lbm.SIDES_PERIODIC, storage="f64", device=dev)
         c64 = lbm.Case(p64)
+        c64.set_step_kernel(kind)
         c64.init_conduction(1000 + rank, 1e-3, stream=stream)
         c64.step(args.warmup, stream=stream)
         barrier(world)
@@ -282,6 +287,7 @@ def run_engine(args):
         "config": {"workload": f"RB {w['lx']}x{w['ly']}x{w['lz']} Ra={w['rayleigh']:.0e} Pr={w['prandtl']} "
                                f"periodic sides, {args.storage} populations",
                    "nodes_per_gpu": nodes, "l2": "state larger than L2 (no flush needed)",
+                   "step_kernel": kernel_used,
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
                 "h2d_bytes_per_step": int(nbytes / args.steps),
@@ -357,6 +363,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "node", "row"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

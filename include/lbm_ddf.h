@@ -57,6 +57,12 @@ extern "C" {
 #define LBM_STORE_F16S 2       /* FP16 of f_i/w_i and g_i/w_i - t0 */
 #define LBM_STORE_BF16S 3      /* BF16 of the same shifted values */
 
+/* step kernels (same results, different data movement) */
+#define LBM_KERNEL_AUTO 0      /* NODE (measured the faster on B200) */
+#define LBM_KERNEL_NODE 1      /* one node per thread, any grid and side-wall mode */
+#define LBM_KERNEL_ROW 2       /* whole x-rows staged by bulk copies; periodic sides,
+                                  32 <= LX <= 256, LX*element size a multiple of 16 bytes */
+
 /* Run surface of src/parameters.h:8-26 plus the engine's own choices. */
 typedef struct lbm_params {
     int32_t lx, ly, lz;        /* LX, LY, LZ (>= 2, 3, 2); y vertical */
@@ -194,6 +200,11 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
  * differ from the GPU's correctly rounded division by `divisor`.  A
  * diagnostic with no counterpart in the reference; expected result 0. */
 int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed, uint64_t *mismatches);
+
+/* Chooses the step kernel of a case (LBM_KERNEL_*); LBM_ERR_ARG if the case
+ * cannot use it.  lbm_get_step_kernel reports the one lbm_step launches. */
+int lbm_set_step_kernel(lbm_case *c, int32_t kind);
+int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
 
 /* Parameters and step count of a case. */
 int lbm_get_params(const lbm_case *c, lbm_params *p, lbm_derived *d, int64_t *step);

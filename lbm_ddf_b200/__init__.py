@@ -30,6 +30,7 @@ SIDES_WALL, SIDES_PERIODIC = 0, 1
 STORE_F64, STORE_F32, STORE_F16S, STORE_BF16S = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORE_F64, "f32": STORE_F32, "f16s": STORE_F16S, "bf16s": STORE_BF16S}
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32: 4, STORE_F16S: 2, STORE_BF16S: 2}
+KERNEL_AUTO, KERNEL_NODE, KERNEL_ROW = 0, 1, 2
 
 
 class LbmError(RuntimeError):
@@ -99,13 +100,15 @@ def lib() -> C.CDLL:
         L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
         L.lbm_save_state.argtypes = [vp, vp, C.c_uint64, vp]
         L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
+        L.lbm_set_step_kernel.argtypes = [vp, C.c_int32]
+        L.lbm_get_step_kernel.argtypes = [vp, C.POINTER(C.c_int32)]
         L.lbm_observables_noalloc.argtypes = [P, vp, vp, vp, C.c_uint64, C.c_int32, C.c_int64, vp, vp]
         L.lbm_selfcheck_division.argtypes = [C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
         for name in ("lbm_derive", "lbm_case_bytes", "lbm_create", "lbm_destroy", "lbm_init_rest",
                      "lbm_init_conduction", "lbm_load_ref_state", "lbm_store_ref_state", "lbm_step",
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
                      "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
-                     "lbm_observables_noalloc"):
+                     "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -287,6 +290,15 @@ class Case:
         if rc != OK and not (allow_diverged and rc == ERR_DIVERGED):
             check(rc)
         return o.as_dict()
+
+    @property
+    def step_kernel(self) -> int:
+        k = C.c_int32()
+        check(lib().lbm_get_step_kernel(self._h, C.byref(k)))
+        return int(k.value)
+
+    def set_step_kernel(self, kind: int):
+        check(lib().lbm_set_step_kernel(self._h, int(kind)))
 
     def checkpoint_bytes(self) -> int:
         b = C.c_uint64()

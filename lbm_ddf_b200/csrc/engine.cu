@@ -21,6 +21,7 @@
 #include <vector>
 
 #include "../../include/lbm_ddf.h"
+#include "rowstep.cuh"
 #include "step.cuh"
 
 using namespace lbm;
@@ -329,6 +330,8 @@ struct lbm_case {
     bool initialised = false;
     bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
     void *f = nullptr, *g = nullptr, *phip = nullptr;
+    int32_t kernel = LBM_KERNEL_AUTO;    // step kernel choice
+    int *d_err = nullptr;                // set by a step kernel whose bulk-copy wait timed out
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
     int obs_blocks = 0;
@@ -426,7 +429,43 @@ template <class S, bool SW, bool PER> void launch_step_t(const StepArgs<S> &a, i
     step_kernel<S, SW, PER><<<grid_for(nodes, kStepThreads), kStepThreads, 0, st>>>(a);
 }
 
+// Whether the row-staged kernel (rowstep.cuh) can run this case.
+bool row_eligible(const lbm_case *c) {
+    const size_t sb = store_bytes(c->p.storage);
+    return c->p.sides == LBM_SIDES_PERIODIC && c->p.lx >= 32 && c->p.lx <= 256 && ((size_t)c->p.lx * sb) % 16 == 0;
+}
+
+// LBM_KERNEL_AUTO runs the node kernel: on B200 it measured faster than the
+// row-staged one (whose bulk copies do not raise the bandwidth the node
+// kernel already reaches); the autotuner may still choose ROW per case.
+bool use_row_kernel(const lbm_case *c) { return c->kernel == LBM_KERNEL_ROW; }
+
+template <class S, bool SW, int PITCH>
+cudaError_t launch_row_p(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    static bool configured = false;   // per instantiation; the attribute is per device function
+    const size_t smem = row_smem_bytes<S>(PITCH);
+    if (!configured) {
+        cudaError_t e = cudaFuncSetAttribute(row_step_kernel<S, SW, PITCH>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+        configured = true;
+    }
+    row_step_kernel<S, SW, PITCH><<<(unsigned)(c->p.ly * c->p.lz), (unsigned)c->p.lx, smem, st>>>(a, c->d_err);
+    return cudaSuccess;
+}
+
+template <class S, bool SW> cudaError_t launch_row_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    if (c->p.lx <= 64) return launch_row_p<S, SW, 64>(c, a, st);
+    if (c->p.lx <= 128) return launch_row_p<S, SW, 128>(c, a, st);
+    return launch_row_p<S, SW, 256>(c, a, st);
+}
+
 template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    if (use_row_kernel(c)) {
+        if (c->swapped) launch_row_t<S, true>(c, a, st);
+        else launch_row_t<S, false>(c, a, st);
+        return;
+    }
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
         if (per) launch_step_t<S, true, true>(a, c->nodes, st);
@@ -508,6 +547,8 @@ int lbm_create(const lbm_params *p, lbm_case **out) {
     if (e == cudaSuccess) e = cudaMalloc(&c->phip, carry_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&c->partial, (size_t)c->obs_blocks * kObs * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_obs, sizeof(lbm_observables));
+    if (e == cudaSuccess) e = cudaMalloc(&c->d_err, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(c->d_err, 0, sizeof(int));
     if (e != cudaSuccess) {
         cudaGetLastError();
         lbm_destroy(c);
@@ -526,6 +567,7 @@ int lbm_destroy(lbm_case *c) {
     cudaFree(c->phip);
     cudaFree(c->partial);
     cudaFree(c->d_obs);
+    cudaFree(c->d_err);
     delete c;
     return LBM_OK;
 }
@@ -713,7 +755,10 @@ int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, c->d_obs, sizeof(lbm_observables), cudaMemcpyDeviceToHost, st));
+    int err = 0;
+    CUDA_TRY(cudaMemcpyAsync(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    if (err) return fail(LBM_ERR_CUDA, "a step kernel gave up waiting for its shared-memory copies");
     if (out->diverged) return fail(LBM_ERR_DIVERGED, "NaN/Inf in the macroscopic fields");
     return LBM_OK;
 }
@@ -922,6 +967,23 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
     cudaFree(d);
     if (e != cudaSuccess) return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
     *mismatches = h;
+    return LBM_OK;
+}
+
+int lbm_set_step_kernel(lbm_case *c, int32_t kind) {
+    if (!c) return fail(LBM_ERR_ARG, "case is NULL");
+    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_NODE && kind != LBM_KERNEL_ROW)
+        return fail(LBM_ERR_ARG, "unknown step kernel");
+    if (kind == LBM_KERNEL_ROW && !row_eligible(c))
+        return fail(LBM_ERR_ARG, "the row-staged kernel needs periodic sides, 32 <= LX <= 256 and LX*element "
+                                 "size a multiple of 16 bytes");
+    c->kernel = kind;
+    return LBM_OK;
+}
+
+int lbm_get_step_kernel(const lbm_case *c, int32_t *kind) {
+    if (!c || !kind) return fail(LBM_ERR_ARG, "NULL argument");
+    *kind = use_row_kernel(c) ? LBM_KERNEL_ROW : LBM_KERNEL_NODE;
     return LBM_OK;
 }
 

@@ -128,25 +128,31 @@ __device__ __forceinline__ bool inside(const Node &g) {
     return (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) && (DY < 0 ? g.vym : DY > 0 ? g.vyp : true) &&
            (DZ < 0 ? g.vzm : DZ > 0 ? g.vzp : true);
 }
+// With INTERIOR set the caller guarantees every neighbour is inside the box
+// (periodic sides and 0 < iy < LY-1), so no test is made.
+template <bool INTERIOR, int DX, int DY, int DZ>
+__device__ __forceinline__ bool inside_t(const Node &g) {
+    return INTERIOR ? true : inside<DX, DY, DZ>(g);
+}
 
 // Population k of node g at the current time, from either layout; rows[k]
 // is the base of population row k.
-template <class S, bool SWAPPED, int K>
+template <class S, bool SWAPPED, int K, bool INTERIOR = false>
 __device__ __forceinline__ S load_pop(S *const (&rows)[Q], const Node &g) {
     if (!SWAPPED) return rows[K][g.n];
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
-    if (inside<DX, DY, DZ>(g)) return rows[opp(K)][(int32_t)g.n + disp<DX, DY, DZ>(g)];
+    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return rows[opp(K)][(int32_t)g.n + disp<DX, DY, DZ>(g)];
     return rows[K][g.n];
 }
 
-template <class S, bool SWAPPED>
+template <class S, bool SWAPPED, bool INTERIOR = false>
 __device__ __forceinline__ void gather(const StepArgs<S> &a, const Node &g, typename Codec<S>::R (&fr)[Q],
                                        typename Codec<S>::R (&gr)[Q]) {
     using C = Codec<S>;
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K>(a.fl, g), a.t0);
-        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K>(a.gl, g), a.t0);
+        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR>(a.fl, g), a.t0);
+        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR>(a.gl, g), a.t0);
     });
 }
 
@@ -300,7 +306,7 @@ __device__ __forceinline__ R abb(R gv, R tw, R rho) {
 
 // Write the post-collision populations of node g to where the next step
 // reads them.  rho is the node's pre-collision density (for anti-bounce-back).
-template <class S, bool SWAPPED, bool PERIODIC>
+template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR = false>
 __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, const typename Codec<S>::R (&fr)[Q],
                                         const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
     using C = Codec<S>;
@@ -310,10 +316,10 @@ __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, con
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
         R fv = fr[I];
         R gv = gr[I];
-        const bool out_y = (DY < 0 && !g.vym) || (DY > 0 && !g.vyp);
+        const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
-        if (SWAPPED && inside<DX, DY, DZ>(g)) {
+        if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
             const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
             a.fs[I][j] = C::template f_out<I>(fv, a.t0);
             a.gs[I][j] = C::template g_out<I>(gv, a.t0);
@@ -336,11 +342,20 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
     if (n >= a.nodes) return;
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
-    gather<S, SWAPPED>(a, g, fr, gr);
+    // Periodic sides: rows away from the plates need no boundary tests.  The
+    // branch is uniform over a warp whenever LX is a multiple of 32.
+    const bool interior = PERIODIC && g.vym && g.vyp;
+    if (interior)
+        gather<S, SWAPPED, true>(a, g, fr, gr);
+    else
+        gather<S, SWAPPED, false>(a, g, fr, gr);
     const Moments<R> m = node_moments(a, fr, gr, n);
     collide<S>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
-    scatter<S, SWAPPED, PERIODIC>(a, g, fr, gr, m.rho);
+    if (interior)
+        scatter<S, SWAPPED, PERIODIC, true>(a, g, fr, gr, m.rho);
+    else
+        scatter<S, SWAPPED, PERIODIC, false>(a, g, fr, gr, m.rho);
 }
 
 }  // namespace lbm

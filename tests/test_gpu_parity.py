@@ -218,6 +218,59 @@ def test_mass_is_conserved(lbm):
     assert abs(m1 - m0) < 1e-13
 
 
+# ---------------------------------------------------------------- row-staged kernel
+
+def _run_kind(lbm, p, steps, kind, seed=9):
+    with lbm.Case(p) as c:
+        c.set_step_kernel(kind)
+        assert c.step_kernel == kind
+        c.init_conduction(seed, 1e-2)
+        c.step(steps)
+        return c.store_ref_state(("f", "g", "uy", "phi")), c.observables()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "bf16s"])
+@pytest.mark.parametrize("lx,ly,lz", [(32, 12, 10), (48, 10, 16), (64, 9, 8)])
+def test_row_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
+    """Same update, different data movement: FP64 bitwise, FP32 to rounding,
+    16-bit storage to a few storage ulps (FP32 fusion choices can differ
+    between the two kernels and flip a 16-bit rounding)."""
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage)
+    a, oa = _run_kind(lbm, p, 5, lbm.KERNEL_NODE)
+    b, ob = _run_kind(lbm, p, 5, lbm.KERNEL_ROW)
+    tol = {"f64": 0.0, "f32": 1e-6, "f16s": 2e-3, "bf16s": 2e-2}[storage]
+    for k in ("f", "g", "phi"):
+        if tol == 0.0:
+            assert np.array_equal(a[k], b[k]), k
+        else:
+            assert relerr(b[k], a[k]) <= tol, k
+
+
+@pytest.mark.parametrize("steps", [1, 2, 7])
+def test_row_kernel_f64_is_bitwise_the_oracle(lbm, oracle_mod, steps):
+    lx, ly, lz = 32, 14, 9
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage="f64")
+    with lbm.Case(p) as c:
+        c.set_step_kernel(lbm.KERNEL_ROW)
+        assert c.step_kernel == lbm.KERNEL_ROW
+        c.init_conduction(5, 1e-3)
+        c.step(steps)
+        got = c.store_ref_state()
+    o = oracle_run(oracle_mod, lx, ly, lz, steps, True, seed=5)
+    compare(got, o, 1e-12, bitwise=True)
+
+
+def test_row_kernel_eligibility(lbm):
+    with lbm.Case(lbm.make_params(40, 8, 8, sides=lbm.SIDES_WALL, storage="f32")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE
+        with pytest.raises(lbm.LbmError):
+            c.set_step_kernel(lbm.KERNEL_ROW)
+    with lbm.Case(lbm.make_params(30, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f32")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE         # 30*4 bytes is not a multiple of 16
+    with lbm.Case(lbm.make_params(512, 4, 4, sides=lbm.SIDES_PERIODIC, storage="f32")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE         # rows longer than 256
+
+
 # ---------------------------------------------------------------- reduced precision
 
 @pytest.mark.parametrize("storage,tol,steps", [("f32", 5e-5, 200), ("f16s", 5e-3, 100), ("bf16s", 4e-2, 100)])
