@@ -116,6 +116,10 @@ int lbm_case_bytes(const lbm_params *p, uint64_t *bytes);
 int lbm_create(const lbm_params *p, lbm_case **out);
 int lbm_destroy(lbm_case *c);
 
+/* The init calls write the state with a kernel on `stream` and return once
+ * it is written (like the reference's synchronous initialize()), so the
+ * case can then be stepped on any stream. */
+
 /* init_arrays, src/initial.cu:208-241: rho = 0, u = 0, phi = 0.5. */
 int lbm_init_rest(lbm_case *c, void *stream);
 
@@ -205,6 +209,35 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
  * cannot use it.  lbm_get_step_kernel reports the one lbm_step launches. */
 int lbm_set_step_kernel(lbm_case *c, int32_t kind);
 int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
+
+/* ---- batches: many cases advanced together ------------------------------
+ * No counterpart in the reference, which runs one case per process.  A batch
+ * holds cases (any grids, Ra, Pr) of one storage format, periodic sides, on
+ * one device; it does not own them.  lbm_batch_step advances every member
+ * by nsteps in one kernel launch per step (a CUDA graph of the launches is
+ * captured on first use of a step count and replayed); each member's step
+ * count and layout advance as with lbm_step, and a member's result is the
+ * same alone or in any mix.  Members stay usable with every single-case
+ * call (observables, profile, store, checkpoint) on the same stream; remove
+ * a case before destroying it.  A case right after lbm_init_rest must take
+ * its first step alone (its first step uses the rest state's phi = 0.5). */
+typedef struct lbm_batch lbm_batch;
+int lbm_batch_create(int device, int32_t storage, lbm_batch **out);
+int lbm_batch_destroy(lbm_batch *b);
+int lbm_batch_add(lbm_batch *b, lbm_case *c);
+int lbm_batch_remove(lbm_batch *b, lbm_case *c);
+int lbm_batch_size(const lbm_batch *b, int32_t *members, uint64_t *nodes);
+int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream);
+/* Launch shape: tile (= block) of 128 or 256 nodes; blocks_per_sm > 0 runs
+ * that many persistent blocks per SM walking the tile list, 0 one block per
+ * tile; use_graph replays captured graphs for multi-step calls. */
+int lbm_batch_set_config(lbm_batch *b, int32_t block, int32_t blocks_per_sm, int32_t use_graph);
+int lbm_batch_get_config(const lbm_batch *b, int32_t *block, int32_t *blocks_per_sm, int32_t *use_graph);
+/* Times every launch shape on 2 x steps_per_trial real steps of the batch
+ * (the shapes compute identical per-node arithmetic, so the steps count),
+ * keeps the fastest and reports it; steps_per_trial must be even. */
+int lbm_batch_autotune(lbm_batch *b, int32_t steps_per_trial, void *stream, int32_t *block,
+                       int32_t *blocks_per_sm, double *best_ms_per_step);
 
 /* Parameters and step count of a case. */
 int lbm_get_params(const lbm_case *c, lbm_params *p, lbm_derived *d, int64_t *step);

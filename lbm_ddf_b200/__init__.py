@@ -102,13 +102,26 @@ def lib() -> C.CDLL:
         L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
         L.lbm_set_step_kernel.argtypes = [vp, C.c_int32]
         L.lbm_get_step_kernel.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.lbm_batch_create.argtypes = [C.c_int, C.c_int32, C.POINTER(vp)]
+        L.lbm_batch_destroy.argtypes = [vp]
+        L.lbm_batch_add.argtypes = [vp, vp]
+        L.lbm_batch_remove.argtypes = [vp, vp]
+        L.lbm_batch_size.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
+        L.lbm_batch_step.argtypes = [vp, C.c_int32, vp]
+        L.lbm_batch_set_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
+        L.lbm_batch_get_config.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
+        L.lbm_batch_autotune.argtypes = [vp, C.c_int32, vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
+                                         C.POINTER(C.c_double)]
         L.lbm_observables_noalloc.argtypes = [P, vp, vp, vp, C.c_uint64, C.c_int32, C.c_int64, vp, vp]
         L.lbm_selfcheck_division.argtypes = [C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.POINTER(C.c_uint64)]
         for name in ("lbm_derive", "lbm_case_bytes", "lbm_create", "lbm_destroy", "lbm_init_rest",
                      "lbm_init_conduction", "lbm_load_ref_state", "lbm_store_ref_state", "lbm_step",
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
                      "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
-                     "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel"):
+                     "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel",
+                     "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
+                     "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
+                     "lbm_batch_autotune"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -320,3 +333,64 @@ class Case:
         out = np.empty(5 * self.params.ly, dtype=np.float64)
         check(lib().lbm_get_profile(self._h, _ptr(out), _stream_handle(stream)))
         return out.reshape(self.params.ly, 5)
+
+
+class Batch:
+    """Cases advanced together by one kernel launch per step (C ABI
+    lbm_batch_*).  The batch does not own its cases."""
+
+    def __init__(self, storage=STORE_F32, device: int = 0):
+        if isinstance(storage, str):
+            storage = STORAGE_NAMES[storage]
+        h = C.c_void_p()
+        check(lib().lbm_batch_create(device, storage, C.byref(h)))
+        self._h = h
+        self.members = []
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().lbm_batch_destroy(self._h)
+            self._h = None
+            self.members = []
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def add(self, case: "Case"):
+        check(lib().lbm_batch_add(self._h, case.handle))
+        self.members.append(case)
+
+    def remove(self, case: "Case"):
+        check(lib().lbm_batch_remove(self._h, case.handle))
+        self.members.remove(case)
+
+    def size(self):
+        m, n = C.c_int32(), C.c_uint64()
+        check(lib().lbm_batch_size(self._h, C.byref(m), C.byref(n)))
+        return int(m.value), int(n.value)
+
+    def step(self, n: int = 1, stream=None):
+        check(lib().lbm_batch_step(self._h, int(n), _stream_handle(stream)))
+
+    def set_config(self, block: int = 128, blocks_per_sm: int = 0, use_graph: bool = True):
+        check(lib().lbm_batch_set_config(self._h, block, blocks_per_sm, int(bool(use_graph))))
+
+    def config(self) -> dict:
+        b, p, g = C.c_int32(), C.c_int32(), C.c_int32()
+        check(lib().lbm_batch_get_config(self._h, C.byref(b), C.byref(p), C.byref(g)))
+        return {"block": b.value, "blocks_per_sm": p.value, "use_graph": bool(g.value)}
+
+    def autotune(self, steps_per_trial: int = 4, stream=None) -> dict:
+        b, p, ms = C.c_int32(), C.c_int32(), C.c_double()
+        check(lib().lbm_batch_autotune(self._h, steps_per_trial, _stream_handle(stream), C.byref(b), C.byref(p),
+                                       C.byref(ms)))
+        return {"block": b.value, "blocks_per_sm": p.value, "ms_per_step": ms.value}

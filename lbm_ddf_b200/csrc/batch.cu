@@ -1,0 +1,424 @@
+// batch.cu — many Rayleigh–Bénard cases advanced together.
+//
+// A batch is a set of cases (any grids, Ra, Pr; one storage format;
+// periodic sides) on one device.  One launch of batch_step_kernel advances
+// every member by one step: the members' nodes are cut into tiles of BLOCK
+// nodes, numbered case after case; blocks walk the tile list with a grid
+// stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block per
+// tile), find each tile's case by a binary search over the tiles' prefix
+// sums held in shared memory, and apply the same node update as the
+// single-case kernel (step.cuh update_node) with that case's parameters and
+// AA layout.  A case's result does not depend on the other members.
+//
+// Repeated steps are captured once into a CUDA graph (one kernel node per
+// step, alternating layouts) and replayed.  The launch shape (block size and
+// grid) is chosen by lbm_batch_autotune, which times each candidate on real
+// steps of the batch: every shape computes the same per-node arithmetic, so
+// no step is wasted.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+#include <new>
+#include <vector>
+
+#include "internal.h"
+#include "step.cuh"
+
+using namespace lbm;
+using namespace lbm_internal;
+
+namespace lbm {
+
+constexpr int kMaxBatch = 2048;    // members per batch (tile prefix sums in shared memory)
+
+// Per-member descriptor, read by every block that works on the member.
+// It provides what update_node needs (the accessor interface of StepArgs).
+template <class S> struct BatchCase {
+    using R = typename Codec<S>::R;
+    using P = typename Codec<S>::P;
+    S *f, *g;            // population row 0; row k at + k*ps
+    S *f_st, *g_st;      // the same arrays, for stores (see StepArgs)
+    P *phip;
+    uint32_t ps, nodes;
+    int32_t lx, ly, lz, swapped;
+    FastDiv div_lx, div_ly;
+    R tau, tauc, rcp_tau, rcp_tauc, rcp_rt;
+    R omega_f, omega_g, force_fac, gb, t0, t_hot, t_cold, phi_fix;
+    int32_t use_phi_fix, pad;
+
+    __device__ __forceinline__ S *ld_row(int which, int k) const { return (which ? g : f) + (size_t)k * ps; }
+    __device__ __forceinline__ S *st_row(int which, int k) const { return (which ? g_st : f_st) + (size_t)k * ps; }
+};
+
+// resident blocks per SM the registers are sized for (<= 128 registers a
+// thread; FP64 holds 54 doubles and gets up to 255)
+template <class S, int BLOCK> struct BatchOccupancy {
+    static constexpr int value = sizeof(S) == 8 ? 256 / BLOCK : 512 / BLOCK;
+};
+
+template <class S, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
+    batch_step_kernel(const BatchCase<S> *__restrict__ cases, int ncases, const uint32_t *__restrict__ tile_start,
+                      uint32_t total_tiles, int parity_flip) {
+    __shared__ uint32_t s_start[kMaxBatch + 1];
+    for (int i = threadIdx.x; i <= ncases; i += BLOCK) s_start[i] = tile_start[i];
+    __syncthreads();
+    for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        int lo = 0, hi = ncases;   // the member c with s_start[c] <= t < s_start[c+1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_start[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        const BatchCase<S> &cs = cases[lo];
+        const uint32_t n = (t - s_start[lo]) * BLOCK + threadIdx.x;
+        if (n < cs.nodes) {
+            if (cs.swapped ^ parity_flip) update_node<S, true, true>(cs, n);
+            else update_node<S, false, true>(cs, n);
+        }
+    }
+}
+
+}  // namespace lbm
+
+struct lbm_batch {
+    int device = 0;
+    int32_t storage = LBM_STORE_F32;
+    std::vector<lbm_case *> members;
+    int32_t block = 128;           // tile size = threads per block
+    int32_t blocks_per_sm = 0;     // 0: one block per tile
+    bool use_graph = true;
+    // device copies of the descriptors and tile prefix sums
+    void *d_cases = nullptr;
+    uint32_t *d_start = nullptr;
+    int capacity = 0;
+    uint32_t total_tiles = 0;
+    bool dirty = true;             // descriptors need rebuilding / uploading
+    std::vector<unsigned char> h_cases;
+    std::vector<uint32_t> h_start;
+    // captured graphs, keyed by the number of steps; dropped when anything changes
+    std::map<int, cudaGraphExec_t> graphs;
+    cudaStream_t capture_stream = nullptr;
+    int sm_count = 148;
+};
+
+namespace {
+
+size_t case_desc_bytes(int storage) {
+    switch (storage) {
+    case LBM_STORE_F64: return sizeof(BatchCase<double>);
+    case LBM_STORE_F32: return sizeof(BatchCase<float>);
+    case LBM_STORE_F16S: return sizeof(BatchCase<__half>);
+    default: return sizeof(BatchCase<__nv_bfloat16>);
+    }
+}
+
+void drop_graphs(lbm_batch *b) {
+    for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+    b->graphs.clear();
+}
+
+template <class S> BatchCase<S> describe(const lbm_case *c) {
+    using R = typename Codec<S>::R;
+    BatchCase<S> d;
+    std::memset(&d, 0, sizeof d);
+    d.f = d.f_st = (S *)c->f;
+    d.g = d.g_st = (S *)c->g;
+    d.phip = (typename Codec<S>::P *)c->phip;
+    d.ps = (uint32_t)c->ps;
+    d.nodes = (uint32_t)c->nodes;
+    d.lx = c->p.lx;
+    d.ly = c->p.ly;
+    d.lz = c->p.lz;
+    d.swapped = c->swapped ? 1 : 0;
+    d.div_lx = FastDiv((uint32_t)c->p.lx);
+    d.div_ly = FastDiv((uint32_t)c->p.ly);
+    d.tau = (R)c->d.tau;
+    d.tauc = (R)c->d.tauc;
+    d.rcp_tau = (R)(1.0 / c->d.tau);
+    d.rcp_tauc = (R)(1.0 / c->d.tauc);
+    d.rcp_rt = (R)(1.0 / (1.0 / 3.0));
+    d.omega_f = (R)(1.0 / c->d.tau);
+    d.omega_g = (R)(1.0 / c->d.tauc);
+    d.force_fac = (R)(1.0 - 0.5 / c->d.tau);
+    d.gb = (R)(c->p.gravity * c->p.beta);
+    d.t0 = (R)c->d.t0;
+    d.t_hot = (R)c->p.t_hot;
+    d.t_cold = (R)c->p.t_cold;
+    d.phi_fix = (R)0.5;
+    d.use_phi_fix = 0;
+    return d;
+}
+
+template <class Fn> int with_batch_storage(const lbm_batch *b, Fn &&fn) {
+    switch (b->storage) {
+    case LBM_STORE_F64: return fn((double *)nullptr);
+    case LBM_STORE_F32: return fn((float *)nullptr);
+    case LBM_STORE_F16S: return fn((__half *)nullptr);
+    case LBM_STORE_BF16S: return fn((__nv_bfloat16 *)nullptr);
+    }
+    return fail(LBM_ERR_ARG, "bad storage");
+}
+
+// Rebuilds and uploads the descriptors if the membership or a layout changed.
+int refresh(lbm_batch *b, cudaStream_t st) {
+    if (!b->dirty) return LBM_OK;
+    const int n = (int)b->members.size();
+    const size_t db = case_desc_bytes(b->storage);
+    if (n > b->capacity) {
+        const int cap = std::max(n, std::max(16, 2 * b->capacity));
+        void *dc = nullptr;
+        uint32_t *ds = nullptr;
+        CUDA_TRY(cudaMalloc(&dc, (size_t)cap * db));
+        cudaError_t e = cudaMalloc(&ds, (size_t)(cap + 1) * sizeof(uint32_t));
+        if (e != cudaSuccess) {
+            cudaFree(dc);
+            return fail(LBM_ERR_NOMEM, "batch descriptor allocation failed");
+        }
+        CUDA_TRY(cudaStreamSynchronize(st));
+        cudaFree(b->d_cases);
+        cudaFree(b->d_start);
+        b->d_cases = dc;
+        b->d_start = ds;
+        b->capacity = cap;
+        drop_graphs(b);
+    }
+    b->h_cases.assign((size_t)n * db, 0);
+    b->h_start.assign((size_t)n + 1, 0);
+    uint32_t tiles = 0;
+    int rc = with_batch_storage(b, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        for (int i = 0; i < n; i++) {
+            const BatchCase<S> d = describe<S>(b->members[i]);
+            std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
+            b->h_start[i] = tiles;
+            tiles += (uint32_t)((b->members[i]->nodes + b->block - 1) / b->block);
+        }
+        return LBM_OK;
+    });
+    if (rc) return rc;
+    b->h_start[n] = tiles;
+    if (tiles != b->total_tiles) drop_graphs(b);
+    b->total_tiles = tiles;
+    if (n > 0) {
+        CUDA_TRY(cudaMemcpyAsync(b->d_cases, b->h_cases.data(), b->h_cases.size(), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(b->d_start, b->h_start.data(), b->h_start.size() * sizeof(uint32_t),
+                                 cudaMemcpyHostToDevice, st));
+        // the host vectors must outlive the copies
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    b->dirty = false;
+    return LBM_OK;
+}
+
+unsigned grid_of(const lbm_batch *b) {
+    if (b->blocks_per_sm <= 0) return b->total_tiles;
+    return (unsigned)std::min<uint64_t>(b->total_tiles, (uint64_t)b->sm_count * b->blocks_per_sm);
+}
+
+// Enqueues `nsteps` batch steps on `st` (parities flip from step to step).
+int enqueue_steps(lbm_batch *b, int nsteps, cudaStream_t st) {
+    const int n = (int)b->members.size();
+    const unsigned grid = grid_of(b);
+    if (grid == 0) return LBM_OK;
+    return with_batch_storage(b, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        const BatchCase<S> *cases = (const BatchCase<S> *)b->d_cases;
+        for (int s = 0; s < nsteps; s++) {
+            if (b->block == 256)
+                batch_step_kernel<S, 256><<<grid, 256, 0, st>>>(cases, n, b->d_start, b->total_tiles, s & 1);
+            else
+                batch_step_kernel<S, 128><<<grid, 128, 0, st>>>(cases, n, b->d_start, b->total_tiles, s & 1);
+        }
+        return LBM_OK;
+    });
+}
+
+void advance_members(lbm_batch *b, int nsteps) {
+    for (lbm_case *c : b->members) {
+        c->step += nsteps;
+        if (nsteps & 1) c->swapped = !c->swapped;
+    }
+    if (nsteps & 1) b->dirty = true;   // layouts changed: descriptors must be rebuilt
+}
+
+}  // namespace
+
+extern "C" {
+
+int lbm_batch_create(int device, int32_t storage, lbm_batch **out) {
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    *out = nullptr;
+    if (store_bytes(storage) == 0) return fail(LBM_ERR_ARG, "bad storage");
+    lbm_batch *b = new (std::nothrow) lbm_batch();
+    if (!b) return fail(LBM_ERR_NOMEM, "host allocation failed");
+    b->device = device;
+    b->storage = storage;
+    DeviceGuard dg(device);
+    cudaError_t e = cudaStreamCreateWithFlags(&b->capture_stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&b->sm_count, cudaDevAttrMultiProcessorCount, device);
+    if (e != cudaSuccess) {
+        delete b;
+        return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    }
+    *out = b;
+    return LBM_OK;
+}
+
+int lbm_batch_destroy(lbm_batch *b) {
+    if (!b) return LBM_OK;
+    DeviceGuard dg(b->device);
+    drop_graphs(b);
+    cudaFree(b->d_cases);
+    cudaFree(b->d_start);
+    if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
+    delete b;
+    return LBM_OK;
+}
+
+int lbm_batch_add(lbm_batch *b, lbm_case *c) {
+    if (!b || !c) return fail(LBM_ERR_ARG, "NULL argument");
+    if (!c->initialised) return fail(LBM_ERR_STATE, "case has no state yet");
+    if (c->p.device != b->device) return fail(LBM_ERR_ARG, "case is on another device");
+    if (c->p.storage != b->storage) return fail(LBM_ERR_ARG, "case storage differs from the batch's");
+    if (c->p.sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "batches run periodic-side cases only");
+    if (c->rest_phi) return fail(LBM_ERR_STATE, "take the first step of a rest-state case alone before batching it");
+    if ((int)b->members.size() >= kMaxBatch) return fail(LBM_ERR_ARG, "batch is full");
+    if (std::find(b->members.begin(), b->members.end(), c) != b->members.end())
+        return fail(LBM_ERR_ARG, "case is already in the batch");
+    b->members.push_back(c);
+    b->dirty = true;
+    drop_graphs(b);
+    return LBM_OK;
+}
+
+int lbm_batch_remove(lbm_batch *b, lbm_case *c) {
+    if (!b || !c) return fail(LBM_ERR_ARG, "NULL argument");
+    auto it = std::find(b->members.begin(), b->members.end(), c);
+    if (it == b->members.end()) return fail(LBM_ERR_ARG, "case is not in the batch");
+    b->members.erase(it);
+    b->dirty = true;
+    drop_graphs(b);
+    return LBM_OK;
+}
+
+int lbm_batch_size(const lbm_batch *b, int32_t *members, uint64_t *nodes) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (members) *members = (int32_t)b->members.size();
+    if (nodes) {
+        uint64_t s = 0;
+        for (const lbm_case *c : b->members) s += (uint64_t)c->nodes;
+        *nodes = s;
+    }
+    return LBM_OK;
+}
+
+int lbm_batch_set_config(lbm_batch *b, int32_t block, int32_t blocks_per_sm, int32_t use_graph) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (block != 128 && block != 256) return fail(LBM_ERR_ARG, "block must be 128 or 256");
+    if (blocks_per_sm < 0 || blocks_per_sm > 64) return fail(LBM_ERR_ARG, "blocks_per_sm must be 0..64");
+    if (block != b->block) b->dirty = true;
+    b->block = block;
+    b->blocks_per_sm = blocks_per_sm;
+    b->use_graph = use_graph != 0;
+    drop_graphs(b);
+    return LBM_OK;
+}
+
+int lbm_batch_get_config(const lbm_batch *b, int32_t *block, int32_t *blocks_per_sm, int32_t *use_graph) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (block) *block = b->block;
+    if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+    if (use_graph) *use_graph = b->use_graph ? 1 : 0;
+    return LBM_OK;
+}
+
+int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (nsteps < 0) return fail(LBM_ERR_ARG, "nsteps < 0");
+    if (nsteps == 0 || b->members.empty()) return LBM_OK;
+    DeviceGuard dg(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = refresh(b, st);
+    if (rc) return rc;
+    if (b->use_graph && nsteps > 1) {
+        auto it = b->graphs.find(nsteps);
+        if (it == b->graphs.end()) {
+            cudaGraph_t g = nullptr;
+            CUDA_TRY(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
+            rc = enqueue_steps(b, nsteps, b->capture_stream);
+            cudaError_t e = cudaStreamEndCapture(b->capture_stream, &g);
+            if (rc) {
+                if (g) cudaGraphDestroy(g);
+                return rc;
+            }
+            if (e != cudaSuccess) return fail(LBM_ERR_CUDA, std::string("graph capture: ") + cudaGetErrorString(e));
+            cudaGraphExec_t x = nullptr;
+            e = cudaGraphInstantiate(&x, g, 0);
+            cudaGraphDestroy(g);
+            if (e != cudaSuccess) return fail(LBM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
+            it = b->graphs.emplace(nsteps, x).first;
+        }
+        CUDA_TRY(cudaGraphLaunch(it->second, st));
+    } else {
+        rc = enqueue_steps(b, nsteps, st);
+        if (rc) return rc;
+        CUDA_TRY(cudaGetLastError());
+    }
+    advance_members(b, nsteps);
+    return LBM_OK;
+}
+
+int lbm_batch_autotune(lbm_batch *b, int32_t steps_per_trial, void *stream, int32_t *block, int32_t *blocks_per_sm,
+                       double *best_ms_per_step) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (steps_per_trial < 2 || (steps_per_trial & 1)) return fail(LBM_ERR_ARG, "steps_per_trial must be even, >= 2");
+    if (b->members.empty()) return fail(LBM_ERR_STATE, "batch is empty");
+    DeviceGuard dg(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int blocks[2] = {128, 256};
+    const int per_sm[5] = {0, 4, 8, 16, 32};
+    cudaEvent_t e0, e1;
+    CUDA_TRY(cudaEventCreate(&e0));
+    CUDA_TRY(cudaEventCreate(&e1));
+    double best = 1e30;
+    int bb = b->block, bp = b->blocks_per_sm;
+    const bool graph = b->use_graph;
+    int rc = LBM_OK;
+    for (int bi = 0; bi < 2 && rc == LBM_OK; bi++)
+        for (int pi = 0; pi < 5 && rc == LBM_OK; pi++) {
+            rc = lbm_batch_set_config(b, blocks[bi], per_sm[pi], graph);
+            if (rc) break;
+            rc = lbm_batch_step(b, steps_per_trial, stream);   // warm-up (and graph capture)
+            if (rc) break;
+            cudaEventRecord(e0, st);
+            rc = lbm_batch_step(b, steps_per_trial, stream);
+            if (rc) break;
+            cudaEventRecord(e1, st);
+            cudaError_t e = cudaEventSynchronize(e1);
+            if (e != cudaSuccess) {
+                rc = fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+                break;
+            }
+            float ms = 0;
+            cudaEventElapsedTime(&ms, e0, e1);
+            if (ms / steps_per_trial < best) {
+                best = ms / steps_per_trial;
+                bb = blocks[bi];
+                bp = per_sm[pi];
+            }
+        }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    rc = lbm_batch_set_config(b, bb, bp, graph);
+    if (rc) return rc;
+    if (block) *block = bb;
+    if (blocks_per_sm) *blocks_per_sm = bp;
+    if (best_ms_per_step) *best_ms_per_step = best;
+    return LBM_OK;
+}
+
+}  // extern "C"

@@ -20,31 +20,22 @@
 #include <string>
 #include <vector>
 
-#include "../../include/lbm_ddf.h"
+#include "internal.h"
 #include "rowstep.cuh"
 #include "step.cuh"
 
 using namespace lbm;
 
 namespace {
-
 thread_local std::string g_last_error;
+}  // namespace
+
+namespace lbm_internal {
 
 int fail(int code, const std::string &msg) {
     g_last_error = msg;
     return code;
 }
-
-#define CUDA_TRY(call)                                                                         \
-    do {                                                                                       \
-        cudaError_t e_ = (call);                                                               \
-        if (e_ != cudaSuccess)                                                                 \
-            return fail(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));     \
-    } while (0)
-
-constexpr int kObs = 13;           // partial sums per block, see obs_kernel
-constexpr int kObsThreads = 256;
-constexpr int kStepThreads = 128;
 
 int64_t round_up(int64_t v, int64_t m) { return (v + m - 1) / m * m; }
 
@@ -58,6 +49,14 @@ size_t store_bytes(int storage) {
     }
 }
 
+}  // namespace lbm_internal
+
+using namespace lbm_internal;
+
+namespace {
+constexpr int kObs = 13;           // partial sums per block, see obs_kernel
+constexpr int kObsThreads = 256;
+constexpr int kStepThreads = 128;
 }  // namespace
 
 // ---------------------------------------------------------------------------
@@ -86,7 +85,7 @@ __global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, d
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
         gather<S, SWAPPED>(a, g, fr, gr);
-        const Moments<R> m = node_moments(a, fr, gr, n);
+        const Moments<R> m = node_moments<S>(a, fr, gr, n);
         const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
         acc[0] += uy * phi;
         acc[1] += ux * ux + uy * uy + uz * uz;
@@ -170,7 +169,7 @@ __global__ void __launch_bounds__(kObsThreads) profile_kernel(const StepArgs<S> 
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
         gather<S, SWAPPED>(a, g, fr, gr);
-        const Moments<R> m = node_moments(a, fr, gr, n);
+        const Moments<R> m = node_moments<S>(a, fr, gr, n);
         acc[0] += (double)m.ux;
         acc[1] += (double)m.uy;
         acc[2] += (double)m.uz;
@@ -212,8 +211,10 @@ __global__ void export_pop_kernel(const StepArgs<S> a, int which, int k, double 
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if (K == k) {
-            const S s = load_pop<S, SWAPPED, K>(which ? a.gl : a.fl, g);
-            v = which ? (double)C::template g_in<K>(s, a.t0) : (double)C::template f_in<K>(s, a.t0);
+            if (which)
+                v = (double)C::template g_in<K>(load_pop<S, SWAPPED, K, false, 1>(a, g), a.t0);
+            else
+                v = (double)C::template f_in<K>(load_pop<S, SWAPPED, K, false, 0>(a, g), a.t0);
         }
     });
     out[n] = v;
@@ -228,7 +229,7 @@ __global__ void export_macro_kernel(const StepArgs<S> a, double *__restrict__ ou
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     gather<S, SWAPPED>(a, g, fr, gr);
-    const Moments<R> m = node_moments(a, fr, gr, n);
+    const Moments<R> m = node_moments<S>(a, fr, gr, n);
     const size_t N = a.nodes;
     out[n] = (double)m.rho;
     out[N + n] = (double)m.ux;
@@ -321,23 +322,9 @@ __global__ void division_check_kernel(double b, double y, uint64_t n, uint64_t k
 // ---------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------
-struct lbm_case {
-    lbm_params p;
-    lbm_derived d;
-    int64_t nodes = 0, ps = 0;
-    int64_t step = 0;
-    bool swapped = false;
-    bool initialised = false;
-    bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
-    void *f = nullptr, *g = nullptr, *phip = nullptr;
-    int32_t kernel = LBM_KERNEL_AUTO;    // step kernel choice
-    int *d_err = nullptr;                // set by a step kernel whose bulk-copy wait timed out
-    double *partial = nullptr;           // obs partial sums
-    lbm_observables *d_obs = nullptr;    // reduced observables (device)
-    int obs_blocks = 0;
-};
 
-namespace {
+
+namespace lbm_internal {
 
 int check_params(const lbm_params *p) {
     if (!p) return fail(LBM_ERR_ARG, "params is NULL");
@@ -362,6 +349,10 @@ void derive(const lbm_params *p, lbm_derived *d) {
     d->tauc = 3.0 * d->diff + 0.5;
     d->t0 = 0.5 * (p->t_cold + p->t_hot);
 }
+
+}  // namespace lbm_internal
+
+namespace {
 
 int obs_blocks_for(int64_t nodes) {
     int64_t b = (nodes + kObsThreads - 1) / kObsThreads;
@@ -398,19 +389,6 @@ template <class S> StepArgs<S> make_args(const lbm_case *c) {
     a.phi_fix = (R)0.5;
     return a;
 }
-
-struct DeviceGuard {
-    int prev = -1;
-    explicit DeviceGuard(int dev) {
-        cudaGetDevice(&prev);
-        if (prev != dev) cudaSetDevice(dev);
-    }
-    ~DeviceGuard() {
-        int cur = -1;
-        cudaGetDevice(&cur);
-        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
-    }
-};
 
 inline unsigned grid_for(int64_t nodes, int threads) { return (unsigned)((nodes + threads - 1) / threads); }
 
@@ -591,6 +569,8 @@ static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, v
     });
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
+    // returns with the state written, so later work on any stream sees it
+    CUDA_TRY(cudaStreamSynchronize(st));
     c->swapped = false;
     c->step = 0;
     c->initialised = true;

@@ -1,0 +1,57 @@
+// internal.h — definitions shared by the engine's translation units
+// (engine.cu: single cases; batch.cu: batches of cases).  Not part of the C ABI.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/lbm_ddf.h"
+
+struct lbm_case {
+    lbm_params p;
+    lbm_derived d;
+    int64_t nodes = 0, ps = 0;
+    int64_t step = 0;
+    bool swapped = false;
+    bool initialised = false;
+    bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
+    void *f = nullptr, *g = nullptr, *phip = nullptr;
+    int32_t kernel = LBM_KERNEL_AUTO;    // step kernel choice
+    int *d_err = nullptr;                // set by a step kernel whose bulk-copy wait timed out
+    double *partial = nullptr;           // obs partial sums
+    lbm_observables *d_obs = nullptr;    // reduced observables (device)
+    int obs_blocks = 0;
+};
+
+namespace lbm_internal {
+
+// records `msg` for lbm_last_error() on this thread and returns `code`
+int fail(int code, const std::string &msg);
+size_t store_bytes(int storage);
+int64_t round_up(int64_t v, int64_t m);
+void derive(const lbm_params *p, lbm_derived *d);
+int check_params(const lbm_params *p);
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        cudaGetDevice(&cur);
+        if (prev >= 0 && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+}  // namespace lbm_internal
+
+#define CUDA_TRY(call)                                                                                   \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess)                                                                           \
+            return lbm_internal::fail(LBM_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)

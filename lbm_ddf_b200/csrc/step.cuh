@@ -73,6 +73,10 @@ template <class S> struct StepArgs {
     // instead of sum(g) (one step after lbm_init_rest).
     int32_t use_phi_fix;
     R phi_fix;
+
+    // population rows: loads (f, g) and stores (f, g)
+    __device__ __forceinline__ S *ld_row(int which, int k) const { return which ? gl[k] : fl[k]; }
+    __device__ __forceinline__ S *st_row(int which, int k) const { return which ? gs[k] : fs[k]; }
 };
 
 // Geometry of one node: coordinates, and node-index displacements to the
@@ -135,24 +139,24 @@ __device__ __forceinline__ bool inside_t(const Node &g) {
     return INTERIOR ? true : inside<DX, DY, DZ>(g);
 }
 
-// Population k of node g at the current time, from either layout; rows[k]
-// is the base of population row k.
-template <class S, bool SWAPPED, int K, bool INTERIOR = false>
-__device__ __forceinline__ S load_pop(S *const (&rows)[Q], const Node &g) {
-    if (!SWAPPED) return rows[K][g.n];
+// Population k (of f when WHICH = 0, of g when 1) of node g at the current
+// time, from either layout.  `a` supplies the row bases: a.ld_row(which, k).
+template <class S, bool SWAPPED, int K, bool INTERIOR = false, int WHICH = 0, class A>
+__device__ __forceinline__ S load_pop(const A &a, const Node &g) {
+    if (!SWAPPED) return a.ld_row(WHICH, K)[g.n];
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
-    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return rows[opp(K)][(int32_t)g.n + disp<DX, DY, DZ>(g)];
-    return rows[K][g.n];
+    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return a.ld_row(WHICH, opp(K))[(int32_t)g.n + disp<DX, DY, DZ>(g)];
+    return a.ld_row(WHICH, K)[g.n];
 }
 
-template <class S, bool SWAPPED, bool INTERIOR = false>
-__device__ __forceinline__ void gather(const StepArgs<S> &a, const Node &g, typename Codec<S>::R (&fr)[Q],
+template <class S, bool SWAPPED, bool INTERIOR = false, class A>
+__device__ __forceinline__ void gather(const A &a, const Node &g, typename Codec<S>::R (&fr)[Q],
                                        typename Codec<S>::R (&gr)[Q]) {
     using C = Codec<S>;
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR>(a.fl, g), a.t0);
-        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR>(a.gl, g), a.t0);
+        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g), a.t0);
+        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g), a.t0);
     });
 }
 
@@ -185,8 +189,8 @@ __device__ __forceinline__ Moments<R> moments(const R (&fr)[Q], const R (&gr)[Q]
     return m;
 }
 
-template <class S>
-__device__ __forceinline__ Moments<typename Codec<S>::R> node_moments(const StepArgs<S> &a,
+template <class S, class A>
+__device__ __forceinline__ Moments<typename Codec<S>::R> node_moments(const A &a,
                                                                      const typename Codec<S>::R (&fr)[Q],
                                                                      const typename Codec<S>::R (&gr)[Q],
                                                                      uint32_t n) {
@@ -284,9 +288,9 @@ __device__ __forceinline__ void collide_exact(double (&fr)[Q], double (&gr)[Q], 
     });
 }
 
-template <class S>
+template <class S, class A>
 __device__ __forceinline__ void collide(typename Codec<S>::R (&fr)[Q], typename Codec<S>::R (&gr)[Q],
-                                        const Moments<typename Codec<S>::R> &m, const StepArgs<S> &a) {
+                                        const Moments<typename Codec<S>::R> &m, const A &a) {
     if constexpr (std::is_same<typename Codec<S>::R, double>::value)
         collide_exact(fr, gr, m, a.tau, a.tauc, a.rcp_tau, a.rcp_tauc, a.rcp_rt, a.force_fac, a.gb, a.t0);
     else
@@ -306,8 +310,8 @@ __device__ __forceinline__ R abb(R gv, R tw, R rho) {
 
 // Write the post-collision populations of node g to where the next step
 // reads them.  rho is the node's pre-collision density (for anti-bounce-back).
-template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR = false>
-__device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, const typename Codec<S>::R (&fr)[Q],
+template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR = false, class A>
+__device__ __forceinline__ void scatter(const A &a, const Node &g, const typename Codec<S>::R (&fr)[Q],
                                         const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
     using C = Codec<S>;
     using R = typename C::R;
@@ -321,11 +325,11 @@ __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, con
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
             const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
-            a.fs[I][j] = C::template f_out<I>(fv, a.t0);
-            a.gs[I][j] = C::template g_out<I>(gv, a.t0);
+            a.st_row(0, I)[j] = C::template f_out<I>(fv, a.t0);
+            a.st_row(1, I)[j] = C::template g_out<I>(gv, a.t0);
         } else {
-            a.fs[opp(I)][g.n] = C::template f_out<I>(fv, a.t0);
-            a.gs[opp(I)][g.n] = C::template g_out<I>(gv, a.t0);
+            a.st_row(0, opp(I))[g.n] = C::template f_out<I>(fv, a.t0);
+            a.st_row(1, opp(I))[g.n] = C::template g_out<I>(gv, a.t0);
         }
     });
 }
@@ -335,11 +339,11 @@ __device__ __forceinline__ void scatter(const StepArgs<S> &a, const Node &g, con
 // FP64, which holds 54 doubles across the collision.
 template <class S> struct StepOccupancy { static constexpr int value = sizeof(S) == 8 ? 2 : 4; };
 
-template <class S, bool SWAPPED, bool PERIODIC>
-__global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
+// The whole update of one node: gather, moments, collision, carried
+// temperature, scatter.
+template <class S, bool SWAPPED, bool PERIODIC, class A>
+__device__ __forceinline__ void update_node(const A &a, uint32_t n) {
     using R = typename Codec<S>::R;
-    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= a.nodes) return;
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     // Periodic sides: rows away from the plates need no boundary tests.  The
@@ -349,13 +353,20 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
         gather<S, SWAPPED, true>(a, g, fr, gr);
     else
         gather<S, SWAPPED, false>(a, g, fr, gr);
-    const Moments<R> m = node_moments(a, fr, gr, n);
+    const Moments<R> m = node_moments<S>(a, fr, gr, n);
     collide<S>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
     if (interior)
         scatter<S, SWAPPED, PERIODIC, true>(a, g, fr, gr, m.rho);
     else
         scatter<S, SWAPPED, PERIODIC, false>(a, g, fr, gr, m.rho);
+}
+
+template <class S, bool SWAPPED, bool PERIODIC>
+__global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
+    const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
+    if (n >= a.nodes) return;
+    update_node<S, SWAPPED, PERIODIC>(a, n);
 }
 
 }  // namespace lbm
