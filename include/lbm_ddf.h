@@ -58,10 +58,12 @@ extern "C" {
 #define LBM_STORE_BF16S 3      /* BF16 of the same shifted values */
 
 /* step kernels (same results, different data movement) */
-#define LBM_KERNEL_AUTO 0      /* NODE (measured the faster on B200) */
+#define LBM_KERNEL_AUTO 0      /* NODE (measured the fastest on B200) */
 #define LBM_KERNEL_NODE 1      /* one node per thread, any grid and side-wall mode */
 #define LBM_KERNEL_ROW 2       /* whole x-rows staged by bulk copies; periodic sides,
                                   32 <= LX <= 256, LX*element size a multiple of 16 bytes */
+#define LBM_KERNEL_PAIR 3      /* two nodes per thread, 32-bit accesses; 16-bit storage,
+                                  periodic sides, even LX */
 
 /* Run surface of src/parameters.h:8-26 plus the engine's own choices. */
 typedef struct lbm_params {

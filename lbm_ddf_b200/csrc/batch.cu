@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "internal.h"
+#include "pair16.cuh"
 #include "step.cuh"
 
 using namespace lbm;
@@ -52,10 +53,15 @@ template <class S> struct BatchCase {
     __device__ __forceinline__ S *st_row(int which, int k) const { return (which ? g_st : f_st) + (size_t)k * ps; }
 };
 
-// resident blocks per SM the registers are sized for (<= 128 registers a
-// thread; FP64 holds 54 doubles and gets up to 255)
+// Whether tiles are BLOCK node pairs processed two nodes per thread
+// (pair16.cuh) rather than BLOCK nodes.  Off: the one-node update measured
+// faster for 16-bit storage too.
+template <class S> constexpr bool batch_pairs() { return false; }
+
+// resident blocks per SM the registers are sized for: <= 128 registers a
+// thread for FP32, <= 168 for the paired 16-bit update, up to 255 for FP64
 template <class S, int BLOCK> struct BatchOccupancy {
-    static constexpr int value = sizeof(S) == 8 ? 256 / BLOCK : 512 / BLOCK;
+    static constexpr int value = sizeof(S) == 8 ? 256 / BLOCK : sizeof(S) == 2 ? (BLOCK == 128 ? 3 : 1) : 512 / BLOCK;
 };
 
 template <class S, int BLOCK>
@@ -73,10 +79,14 @@ __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
             else hi = mid;
         }
         const BatchCase<S> &cs = cases[lo];
-        const uint32_t n = (t - s_start[lo]) * BLOCK + threadIdx.x;
-        if (n < cs.nodes) {
-            if (cs.swapped ^ parity_flip) update_node<S, true, true>(cs, n);
-            else update_node<S, false, true>(cs, n);
+        const uint32_t u = (t - s_start[lo]) * BLOCK + threadIdx.x;
+        if constexpr (batch_pairs<S>()) {
+            // every lane calls update_pair (it shuffles across the warp)
+            if (cs.swapped ^ parity_flip) update_pair<S, true>(cs, u);
+            else update_pair<S, false>(cs, u);
+        } else if (u < cs.nodes) {
+            if (cs.swapped ^ parity_flip) update_node<S, true, true>(cs, u);
+            else update_node<S, false, true>(cs, u);
         }
     }
 }
@@ -194,7 +204,8 @@ int refresh(lbm_batch *b, cudaStream_t st) {
             const BatchCase<S> d = describe<S>(b->members[i]);
             std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
             b->h_start[i] = tiles;
-            tiles += (uint32_t)((b->members[i]->nodes + b->block - 1) / b->block);
+            const int64_t units = batch_pairs<S>() ? b->members[i]->nodes / 2 : b->members[i]->nodes;
+            tiles += (uint32_t)((units + b->block - 1) / b->block);
         }
         return LBM_OK;
     });
@@ -285,6 +296,8 @@ int lbm_batch_add(lbm_batch *b, lbm_case *c) {
     if (c->p.storage != b->storage) return fail(LBM_ERR_ARG, "case storage differs from the batch's");
     if (c->p.sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "batches run periodic-side cases only");
     if (c->rest_phi) return fail(LBM_ERR_STATE, "take the first step of a rest-state case alone before batching it");
+    if (batch_pairs<__half>() && store_bytes(c->p.storage) == 2 && (c->p.lx % 2) != 0)
+        return fail(LBM_ERR_ARG, "16-bit batches take cases with an even LX (two nodes per thread)");
     if ((int)b->members.size() >= kMaxBatch) return fail(LBM_ERR_ARG, "batch is full");
     if (std::find(b->members.begin(), b->members.end(), c) != b->members.end())
         return fail(LBM_ERR_ARG, "case is already in the batch");

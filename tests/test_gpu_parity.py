@@ -246,6 +246,36 @@ def test_row_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
             assert relerr(b[k], a[k]) <= tol, k
 
 
+@pytest.mark.parametrize("storage", ["f16s", "bf16s"])
+@pytest.mark.parametrize("lx,ly,lz", [(64, 12, 10), (48, 10, 16), (34, 9, 8), (6, 7, 5), (2, 5, 4)])
+def test_pair_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
+    """Two nodes per thread (16-bit storage): same results as the node
+    kernel, on rows whose pairs fill whole warps and on rows where warps
+    straddle rows (x-shift realigned across lanes and at row ends)."""
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage)
+    a, oa = _run_kind(lbm, p, 6, lbm.KERNEL_NODE)
+    b, ob = _run_kind(lbm, p, 6, lbm.KERNEL_PAIR)
+    tol = {"f16s": 2e-3, "bf16s": 2e-2}[storage]
+    for k in ("f", "g", "phi"):
+        assert relerr(b[k], a[k]) <= tol, k
+    # nearly every stored value agrees bit for bit (the two kernels may fuse
+    # FP32 multiply-adds differently, flipping a rare 16-bit rounding)
+    assert np.mean(a["f"] == b["f"]) > 0.95
+
+
+def test_pair_kernel_eligibility(lbm):
+    with lbm.Case(lbm.make_params(32, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f16s")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE          # the default
+        c.set_step_kernel(lbm.KERNEL_PAIR)
+        assert c.step_kernel == lbm.KERNEL_PAIR
+    with lbm.Case(lbm.make_params(33, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f16s")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE          # odd LX
+        with pytest.raises(lbm.LbmError):
+            c.set_step_kernel(lbm.KERNEL_PAIR)
+    with lbm.Case(lbm.make_params(32, 8, 8, sides=lbm.SIDES_WALL, storage="bf16s")) as c:
+        assert c.step_kernel == lbm.KERNEL_NODE          # closed box
+
+
 @pytest.mark.parametrize("steps", [1, 2, 7])
 def test_row_kernel_f64_is_bitwise_the_oracle(lbm, oracle_mod, steps):
     lx, ly, lz = 32, 14, 9
