@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define LBM_DDF_ABI_VERSION 1
+#define LBM_DDF_ABI_VERSION 2
 
 /* status codes */
 #define LBM_OK 0
@@ -64,6 +64,12 @@ extern "C" {
                                   32 <= LX <= 256, LX*element size a multiple of 16 bytes */
 #define LBM_KERNEL_PAIR 3      /* two nodes per thread, 32-bit accesses; 16-bit storage,
                                   periodic sides, even LX */
+
+/* collision models */
+#define LBM_COLLISION_BGK 0          /* the reference's BGK (src/collision.cu:3-88); default */
+#define LBM_COLLISION_REGULARIZED 1  /* regularised BGK (Latt and Chopard 2006): the relaxed
+                                        non-equilibrium part projected on its second (f) and
+                                        first (g) Hermite moments; same equilibria and force */
 
 /* Run surface of src/parameters.h:8-26 plus the engine's own choices. */
 typedef struct lbm_params {
@@ -212,6 +218,13 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
 int lbm_set_step_kernel(lbm_case *c, int32_t kind);
 int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
 
+/* Chooses the collision model of a case (LBM_COLLISION_*; BGK at creation),
+ * in effect from its next step.  The regularised model runs on the node
+ * kernel (and in batches); LBM_ERR_ARG if the case's step kernel is set to
+ * ROW or PAIR.  No counterpart in the reference, which has BGK only. */
+int lbm_set_collision(lbm_case *c, int32_t model);
+int lbm_get_collision(const lbm_case *c, int32_t *model);
+
 /* ---- batches: many cases advanced together ------------------------------
  * No counterpart in the reference, which runs one case per process.  A batch
  * holds cases (any grids, Ra, Pr) of one storage format, periodic sides, on
@@ -219,10 +232,14 @@ int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
  * by nsteps in one kernel launch per step (a CUDA graph of the launches is
  * captured on first use of a step count and replayed); each member's step
  * count and layout advance as with lbm_step, and a member's result is the
- * same alone or in any mix.  Members stay usable with every single-case
- * call (observables, profile, store, checkpoint) on the same stream; remove
- * a case before destroying it.  A case right after lbm_init_rest must take
- * its first step alone (its first step uses the rest state's phi = 0.5). */
+ * same alone or in any mix; members may differ in collision model.  A case
+ * belongs to at most one batch.  Members stay usable with the single-case
+ * calls that read them (observables, profile, store, save) on the same
+ * stream; the calls that change a case's state or settings (init, load,
+ * lbm_step, restore, lbm_set_collision) return LBM_ERR_STATE for a member
+ * until it is removed.  Destroying a member removes it from its batch.  A
+ * case right after lbm_init_rest must take its first step alone (its first
+ * step uses the rest state's phi = 0.5). */
 typedef struct lbm_batch lbm_batch;
 int lbm_batch_create(int device, int32_t storage, lbm_batch **out);
 int lbm_batch_destroy(lbm_batch *b);

@@ -31,6 +31,8 @@ STORE_F64, STORE_F32, STORE_F16S, STORE_BF16S = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORE_F64, "f32": STORE_F32, "f16s": STORE_F16S, "bf16s": STORE_BF16S}
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32: 4, STORE_F16S: 2, STORE_BF16S: 2}
 KERNEL_AUTO, KERNEL_NODE, KERNEL_ROW, KERNEL_PAIR = 0, 1, 2, 3
+COLLISION_BGK, COLLISION_REGULARIZED = 0, 1
+COLLISION_NAMES = {"bgk": COLLISION_BGK, "regularized": COLLISION_REGULARIZED}
 
 
 class LbmError(RuntimeError):
@@ -102,6 +104,8 @@ def lib() -> C.CDLL:
         L.lbm_restore_state.argtypes = [vp, vp, C.c_uint64, vp]
         L.lbm_set_step_kernel.argtypes = [vp, C.c_int32]
         L.lbm_get_step_kernel.argtypes = [vp, C.POINTER(C.c_int32)]
+        L.lbm_set_collision.argtypes = [vp, C.c_int32]
+        L.lbm_get_collision.argtypes = [vp, C.POINTER(C.c_int32)]
         L.lbm_batch_create.argtypes = [C.c_int, C.c_int32, C.POINTER(vp)]
         L.lbm_batch_destroy.argtypes = [vp]
         L.lbm_batch_add.argtypes = [vp, vp]
@@ -119,6 +123,7 @@ def lib() -> C.CDLL:
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
                      "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
                      "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel",
+                     "lbm_set_collision", "lbm_get_collision",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
                      "lbm_batch_autotune"):
@@ -312,6 +317,16 @@ class Case:
 
     def set_step_kernel(self, kind: int):
         check(lib().lbm_set_step_kernel(self._h, int(kind)))
+
+    @property
+    def collision(self) -> str:
+        m = C.c_int32()
+        check(lib().lbm_get_collision(self._h, C.byref(m)))
+        return next(k for k, v in COLLISION_NAMES.items() if v == m.value)
+
+    def set_collision(self, model):
+        """'bgk' (the reference's collision, the default) or 'regularized'."""
+        check(lib().lbm_set_collision(self._h, COLLISION_NAMES.get(model, model)))
 
     def checkpoint_bytes(self) -> int:
         b = C.c_uint64()

@@ -1,16 +1,20 @@
 // batch.cu — many Rayleigh–Bénard cases advanced together.
 //
-// A batch is a set of cases (any grids, Ra, Pr; one storage format;
-// periodic sides) on one device.  One launch of batch_step_kernel advances
-// every member by one step: the members' nodes are cut into tiles of BLOCK
-// nodes, numbered case after case; blocks walk the tile list with a grid
-// stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block per
-// tile), find each tile's case by a binary search over the tiles' prefix
+// A batch is a set of cases (any grids, Ra, Pr, collision models; one
+// storage format; periodic sides) on one device.  The members are grouped by
+// AA layout and collision model; one launch of batch_step_kernel per
+// non-empty group (normally one: members move through the layouts in step)
+// advances the group's members by one step.  Their nodes are cut into tiles
+// of BLOCK nodes, numbered case after case; blocks walk the tile list with a
+// grid stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block
+// per tile), find each tile's case by a binary search over the tiles' prefix
 // sums held in shared memory, and apply the same node update as the
-// single-case kernel (step.cuh update_node) with that case's parameters and
-// AA layout.  A case's result does not depend on the other members.
+// single-case kernel (step.cuh update_node) with that case's parameters.  A
+// kernel instance holds the code of one layout and one model only, so it
+// needs no more registers than the single-case kernel.  A case's result
+// does not depend on the other members.
 //
-// Repeated steps are captured once into a CUDA graph (one kernel node per
+// Repeated steps are captured once into a CUDA graph (the launches of every
 // step, alternating layouts) and replayed.  The launch shape (block size and
 // grid) is chosen by lbm_batch_autotune, which times each candidate on real
 // steps of the batch: every shape computes the same per-node arithmetic, so
@@ -24,7 +28,7 @@
 #include <vector>
 
 #include "internal.h"
-#include "pair16.cuh"
+#include "step.cuh"
 #include "step.cuh"
 
 using namespace lbm;
@@ -49,29 +53,40 @@ template <class S> struct BatchCase {
     R omega_f, omega_g, force_fac, gb, t0, t_hot, t_cold, phi_fix;
     int32_t use_phi_fix, pad;
 
-    __device__ __forceinline__ S *ld_row(int which, int k) const { return (which ? g : f) + (size_t)k * ps; }
-    __device__ __forceinline__ S *st_row(int which, int k) const { return (which ? g_st : f_st) + (size_t)k * ps; }
+    // element k * ps + j of the population array, indexed in 32 bits (a
+    // member has 27 ps < 2^32 elements per array): one multiply-add per
+    // access and no 64-bit row addresses held in registers
+    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const {
+        return (which ? g : f)[(uint32_t)k * ps + (uint32_t)j];
+    }
+    template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const {
+        return (which ? g_st : f_st)[(uint32_t)k * ps + (uint32_t)j];
+    }
 };
 
-// Whether tiles are BLOCK node pairs processed two nodes per thread
-// (pair16.cuh) rather than BLOCK nodes.  Off: the one-node update measured
-// faster for 16-bit storage too.
-template <class S> constexpr bool batch_pairs() { return false; }
-
-// resident blocks per SM the registers are sized for: <= 128 registers a
-// thread for FP32, <= 168 for the paired 16-bit update, up to 255 for FP64
+// Resident threads per SM the batch kernel's registers are sized for: those
+// of the single-case kernel, except 640 for 16-bit storage (96 registers: the
+// members' parameters come from a descriptor in memory rather than from the
+// constant bank, and the swapped-layout update spills at 80).
+template <class S> constexpr int batch_threads_per_sm() {
+    return sizeof(S) == 2 ? 640 : StepOccupancy<S>::value * 128;
+}
 template <class S, int BLOCK> struct BatchOccupancy {
-    static constexpr int value = sizeof(S) == 8 ? 256 / BLOCK : sizeof(S) == 2 ? (BLOCK == 128 ? 3 : 1) : 512 / BLOCK;
+    static constexpr int value = batch_threads_per_sm<S>() / BLOCK > 0 ? batch_threads_per_sm<S>() / BLOCK : 1;
 };
 
-template <class S, int BLOCK>
+// Advances the members cases[0 .. ncases) of one group, all in layout
+// SWAPPED and collision model COLL, by one step.  tile_start[i] is the first
+// tile of member i (tile numbers are batch-wide; the group owns tiles
+// [tile_start[0], tile_start[ncases])).
+template <class S, int BLOCK, bool SWAPPED, int COLL>
 __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
-    batch_step_kernel(const BatchCase<S> *__restrict__ cases, int ncases, const uint32_t *__restrict__ tile_start,
-                      uint32_t total_tiles, int parity_flip) {
+    batch_step_kernel(const BatchCase<S> *__restrict__ cases, int ncases, const uint32_t *__restrict__ tile_start) {
     __shared__ uint32_t s_start[kMaxBatch + 1];
     for (int i = threadIdx.x; i <= ncases; i += BLOCK) s_start[i] = tile_start[i];
     __syncthreads();
-    for (uint32_t t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    const uint32_t end = s_start[ncases];
+    for (uint32_t t = s_start[0] + blockIdx.x; t < end; t += gridDim.x) {
         int lo = 0, hi = ncases;   // the member c with s_start[c] <= t < s_start[c+1]
         while (hi - lo > 1) {
             const int mid = (lo + hi) >> 1;
@@ -80,14 +95,7 @@ __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
         }
         const BatchCase<S> &cs = cases[lo];
         const uint32_t u = (t - s_start[lo]) * BLOCK + threadIdx.x;
-        if constexpr (batch_pairs<S>()) {
-            // every lane calls update_pair (it shuffles across the warp)
-            if (cs.swapped ^ parity_flip) update_pair<S, true>(cs, u);
-            else update_pair<S, false>(cs, u);
-        } else if (u < cs.nodes) {
-            if (cs.swapped ^ parity_flip) update_node<S, true, true>(cs, u);
-            else update_node<S, false, true>(cs, u);
-        }
+        if (u < cs.nodes) update_node<S, SWAPPED, true, COLL>(cs, u);
     }
 }
 
@@ -104,11 +112,16 @@ struct lbm_batch {
     void *d_cases = nullptr;
     uint32_t *d_start = nullptr;
     int capacity = 0;
-    uint32_t total_tiles = 0;
+    // Member groups (descriptor order): bit 0 = the member's layout differs
+    // from the batch's phase, bit 1 = regularised collision.  Every step
+    // flips all layouts and the phase together, so groups stay fixed.
+    int group_first[4] = {0, 0, 0, 0}, group_count[4] = {0, 0, 0, 0};
+    int phase = 0;
     bool dirty = true;             // descriptors need rebuilding / uploading
     std::vector<unsigned char> h_cases;
     std::vector<uint32_t> h_start;
-    // captured graphs, keyed by the number of steps; dropped when anything changes
+    // captured graphs, keyed by 2 x the number of steps + the phase at
+    // capture; dropped when the membership or the launch shape changes
     std::map<int, cudaGraphExec_t> graphs;
     cudaStream_t capture_stream = nullptr;
     int sm_count = 148;
@@ -172,7 +185,11 @@ template <class Fn> int with_batch_storage(const lbm_batch *b, Fn &&fn) {
     return fail(LBM_ERR_ARG, "bad storage");
 }
 
-// Rebuilds and uploads the descriptors if the membership or a layout changed.
+int group_of(const lbm_batch *b, const lbm_case *c) {
+    return ((c->swapped ? 1 : 0) ^ b->phase) | (c->collision == LBM_COLLISION_REGULARIZED ? 2 : 0);
+}
+
+// Rebuilds and uploads the descriptors after a membership change.
 int refresh(lbm_batch *b, cudaStream_t st) {
     if (!b->dirty) return LBM_OK;
     const int n = (int)b->members.size();
@@ -195,24 +212,29 @@ int refresh(lbm_batch *b, cudaStream_t st) {
         b->capacity = cap;
         drop_graphs(b);
     }
+    std::vector<const lbm_case *> order;
+    order.reserve((size_t)n);
+    for (int g = 0; g < 4; g++) {
+        b->group_first[g] = (int)order.size();
+        for (const lbm_case *c : b->members)
+            if (group_of(b, c) == g) order.push_back(c);
+        b->group_count[g] = (int)order.size() - b->group_first[g];
+    }
     b->h_cases.assign((size_t)n * db, 0);
     b->h_start.assign((size_t)n + 1, 0);
     uint32_t tiles = 0;
     int rc = with_batch_storage(b, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         for (int i = 0; i < n; i++) {
-            const BatchCase<S> d = describe<S>(b->members[i]);
+            const BatchCase<S> d = describe<S>(order[(size_t)i]);
             std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
             b->h_start[i] = tiles;
-            const int64_t units = batch_pairs<S>() ? b->members[i]->nodes / 2 : b->members[i]->nodes;
-            tiles += (uint32_t)((units + b->block - 1) / b->block);
+            tiles += (uint32_t)((order[(size_t)i]->nodes + b->block - 1) / b->block);
         }
         return LBM_OK;
     });
     if (rc) return rc;
     b->h_start[n] = tiles;
-    if (tiles != b->total_tiles) drop_graphs(b);
-    b->total_tiles = tiles;
     if (n > 0) {
         CUDA_TRY(cudaMemcpyAsync(b->d_cases, b->h_cases.data(), b->h_cases.size(), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemcpyAsync(b->d_start, b->h_start.data(), b->h_start.size() * sizeof(uint32_t),
@@ -224,38 +246,67 @@ int refresh(lbm_batch *b, cudaStream_t st) {
     return LBM_OK;
 }
 
-unsigned grid_of(const lbm_batch *b) {
-    if (b->blocks_per_sm <= 0) return b->total_tiles;
-    return (unsigned)std::min<uint64_t>(b->total_tiles, (uint64_t)b->sm_count * b->blocks_per_sm);
+unsigned grid_of(const lbm_batch *b, uint32_t tiles) {
+    if (b->blocks_per_sm <= 0) return tiles;
+    return (unsigned)std::min<uint64_t>(tiles, (uint64_t)b->sm_count * b->blocks_per_sm);
 }
 
-// Enqueues `nsteps` batch steps on `st` (parities flip from step to step).
+template <class S, int BLOCK, bool SW>
+void launch_group(const BatchCase<S> *cases, int n, const uint32_t *start, bool reg, unsigned grid, cudaStream_t st) {
+    if (reg) batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_REGULARIZED><<<grid, BLOCK, 0, st>>>(cases, n, start);
+    else batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
+}
+
+// Enqueues `nsteps` batch steps on `st`: per step one launch per non-empty
+// group, in the layout its members are in at that step.
 int enqueue_steps(lbm_batch *b, int nsteps, cudaStream_t st) {
-    const int n = (int)b->members.size();
-    const unsigned grid = grid_of(b);
-    if (grid == 0) return LBM_OK;
     return with_batch_storage(b, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const BatchCase<S> *cases = (const BatchCase<S> *)b->d_cases;
-        for (int s = 0; s < nsteps; s++) {
-            if (b->block == 256)
-                batch_step_kernel<S, 256><<<grid, 256, 0, st>>>(cases, n, b->d_start, b->total_tiles, s & 1);
-            else
-                batch_step_kernel<S, 128><<<grid, 128, 0, st>>>(cases, n, b->d_start, b->total_tiles, s & 1);
-        }
+        for (int s = 0; s < nsteps; s++)
+            for (int g = 0; g < 4; g++) {
+                const int first = b->group_first[g], n = b->group_count[g];
+                if (n == 0) continue;
+                const uint32_t tiles = b->h_start[first + n] - b->h_start[first];
+                const unsigned grid = grid_of(b, tiles);
+                if (grid == 0) continue;
+                const bool sw = ((g & 1) ^ b->phase ^ (s & 1)) != 0;
+                const bool reg = (g & 2) != 0;
+                const BatchCase<S> *c0 = cases + first;
+                const uint32_t *s0 = b->d_start + first;
+                if (b->block == 256) {
+                    if (sw) launch_group<S, 256, true>(c0, n, s0, reg, grid, st);
+                    else launch_group<S, 256, false>(c0, n, s0, reg, grid, st);
+                } else {
+                    if (sw) launch_group<S, 128, true>(c0, n, s0, reg, grid, st);
+                    else launch_group<S, 128, false>(c0, n, s0, reg, grid, st);
+                }
+            }
         return LBM_OK;
     });
 }
 
+// Every member's layout and the batch phase flip together on odd counts,
+// so the groups and descriptors stay valid.
 void advance_members(lbm_batch *b, int nsteps) {
     for (lbm_case *c : b->members) {
         c->step += nsteps;
         if (nsteps & 1) c->swapped = !c->swapped;
     }
-    if (nsteps & 1) b->dirty = true;   // layouts changed: descriptors must be rebuilt
+    if (nsteps & 1) b->phase ^= 1;
 }
 
 }  // namespace
+
+void lbm_internal::batch_forget(lbm_batch *b, lbm_case *c) {
+    auto it = std::find(b->members.begin(), b->members.end(), c);
+    if (it != b->members.end()) {
+        b->members.erase(it);
+        b->dirty = true;
+        drop_graphs(b);
+    }
+    c->batch = nullptr;
+}
 
 extern "C" {
 
@@ -280,6 +331,7 @@ int lbm_batch_create(int device, int32_t storage, lbm_batch **out) {
 
 int lbm_batch_destroy(lbm_batch *b) {
     if (!b) return LBM_OK;
+    for (lbm_case *m : b->members) m->batch = nullptr;
     DeviceGuard dg(b->device);
     drop_graphs(b);
     cudaFree(b->d_cases);
@@ -296,12 +348,12 @@ int lbm_batch_add(lbm_batch *b, lbm_case *c) {
     if (c->p.storage != b->storage) return fail(LBM_ERR_ARG, "case storage differs from the batch's");
     if (c->p.sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "batches run periodic-side cases only");
     if (c->rest_phi) return fail(LBM_ERR_STATE, "take the first step of a rest-state case alone before batching it");
-    if (batch_pairs<__half>() && store_bytes(c->p.storage) == 2 && (c->p.lx % 2) != 0)
-        return fail(LBM_ERR_ARG, "16-bit batches take cases with an even LX (two nodes per thread)");
+    if (c->batch) return fail(LBM_ERR_ARG, c->batch == b ? "case is already in the batch" : "case is in another batch");
+    if ((uint64_t)Q * (uint64_t)c->ps >= (1ull << 32))
+        return fail(LBM_ERR_ARG, "case too large for a batch (27 x padded nodes must stay below 2^32)");
     if ((int)b->members.size() >= kMaxBatch) return fail(LBM_ERR_ARG, "batch is full");
-    if (std::find(b->members.begin(), b->members.end(), c) != b->members.end())
-        return fail(LBM_ERR_ARG, "case is already in the batch");
     b->members.push_back(c);
+    c->batch = b;
     b->dirty = true;
     drop_graphs(b);
     return LBM_OK;
@@ -312,6 +364,7 @@ int lbm_batch_remove(lbm_batch *b, lbm_case *c) {
     auto it = std::find(b->members.begin(), b->members.end(), c);
     if (it == b->members.end()) return fail(LBM_ERR_ARG, "case is not in the batch");
     b->members.erase(it);
+    c->batch = nullptr;
     b->dirty = true;
     drop_graphs(b);
     return LBM_OK;
@@ -357,7 +410,8 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
     int rc = refresh(b, st);
     if (rc) return rc;
     if (b->use_graph && nsteps > 1) {
-        auto it = b->graphs.find(nsteps);
+        const int key = 2 * nsteps + b->phase;
+        auto it = b->graphs.find(key);
         if (it == b->graphs.end()) {
             cudaGraph_t g = nullptr;
             CUDA_TRY(cudaStreamBeginCapture(b->capture_stream, cudaStreamCaptureModeThreadLocal));
@@ -372,7 +426,7 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
             e = cudaGraphInstantiate(&x, g, 0);
             cudaGraphDestroy(g);
             if (e != cudaSuccess) return fail(LBM_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(e));
-            it = b->graphs.emplace(nsteps, x).first;
+            it = b->graphs.emplace(key, x).first;
         }
         CUDA_TRY(cudaGraphLaunch(it->second, st));
     } else {

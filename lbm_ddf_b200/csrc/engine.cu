@@ -85,7 +85,13 @@ __global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, d
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < a.nodes; n += gridDim.x * blockDim.x) {
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
-        gather<S, SWAPPED>(a, g, fr, gr);
+        // rows away from the plates of a periodic box: no boundary tests
+        // (uniform over a warp whenever LX is a multiple of 32); FP64 keeps
+        // one path (two do not fit its registers)
+        if (sizeof(S) < 8 && SWAPPED && PERIODIC && g.vym && g.vyp)
+            gather<S, SWAPPED, true>(a, g, fr, gr);
+        else
+            gather<S, SWAPPED, false>(a, g, fr, gr);
         const Moments<R> m = node_moments<S>(a, fr, gr, n);
         const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
         acc[0] += uy * phi;
@@ -123,17 +129,19 @@ struct ObsConsts {
     int64_t step;
 };
 
-// Sums the block partials in a fixed order (deterministic) and forms the
-// observables: Nu_bulk of src/output.cu:228-233; Nu_top/bottom of :236-256
-// written with plane sums, <(3T0 - 4T1 + T2)/2> = (3<T0> - 4<T1> + <T2>)/2.
-__global__ void obs_finalize(const double *__restrict__ partial, int nblocks, ObsConsts c,
-                             lbm_observables *__restrict__ out) {
+// Sums the block partials in a fixed order (deterministic: warp w sums
+// quantity w, lane l the blocks l, l + 32, ..., then a butterfly over the
+// lanes) and forms the observables: Nu_bulk of src/output.cu:228-233;
+// Nu_top/bottom of :236-256 written with plane sums,
+// <(3T0 - 4T1 + T2)/2> = (3<T0> - 4<T1> + <T2>)/2.  Launch: kObs warps.
+__global__ void __launch_bounds__(32 * kObs) obs_finalize(const double *__restrict__ partial, int nblocks,
+                                                          ObsConsts c, lbm_observables *__restrict__ out) {
     __shared__ double tot[kObs];
-    if (threadIdx.x < kObs) {
-        double s = 0.0;
-        for (int b = 0; b < nblocks; b++) s += partial[(size_t)b * kObs + threadIdx.x];
-        tot[threadIdx.x] = s;
-    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int b = lane; b < nblocks; b += 32) s += partial[(size_t)b * kObs + w];
+    s = warp_sum(s);
+    if (lane == 0) tot[w] = s;
     __syncthreads();
     if (threadIdx.x == 0) {
         const double uyT = tot[0] / c.nodes;
@@ -404,8 +412,12 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
     return fail(LBM_ERR_ARG, "bad storage");
 }
 
-template <class S, bool SW, bool PER> void launch_step_t(const StepArgs<S> &a, int64_t nodes, cudaStream_t st) {
-    step_kernel<S, SW, PER><<<grid_for(nodes, kStepThreads), kStepThreads, 0, st>>>(a);
+template <class S, bool SW, bool PER> void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    const unsigned grid = grid_for(c->nodes, kStepThreads);
+    if (c->collision == LBM_COLLISION_REGULARIZED)
+        step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED><<<grid, kStepThreads, 0, st>>>(a);
+    else
+        step_kernel<S, SW, PER, LBM_COLLISION_BGK><<<grid, kStepThreads, 0, st>>>(a);
 }
 
 // Whether the row-staged kernel (rowstep.cuh) can run this case.
@@ -468,11 +480,11 @@ template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cud
     }
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
-        if (per) launch_step_t<S, true, true>(a, c->nodes, st);
-        else launch_step_t<S, true, false>(a, c->nodes, st);
+        if (per) launch_step_t<S, true, true>(c, a, st);
+        else launch_step_t<S, true, false>(c, a, st);
     } else {
-        if (per) launch_step_t<S, false, true>(a, c->nodes, st);
-        else launch_step_t<S, false, false>(a, c->nodes, st);
+        if (per) launch_step_t<S, false, true>(c, a, st);
+        else launch_step_t<S, false, false>(c, a, st);
     }
 }
 
@@ -492,6 +504,15 @@ template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cud
 int check_case(const lbm_case *c, bool need_state) {
     if (!c) return fail(LBM_ERR_ARG, "case is NULL");
     if (need_state && !c->initialised) return fail(LBM_ERR_STATE, "case has no state yet (init or load first)");
+    return LBM_OK;
+}
+
+// Calls that change a case's state or layout: not while it is a batch
+// member (the batch's descriptors and captured graphs describe its layout).
+int check_mutable(const lbm_case *c, bool need_state) {
+    const int rc = check_case(c, need_state);
+    if (rc) return rc;
+    if (c->batch) return fail(LBM_ERR_STATE, "case is a batch member: remove it from the batch first");
     return LBM_OK;
 }
 
@@ -561,6 +582,7 @@ int lbm_create(const lbm_params *p, lbm_case **out) {
 
 int lbm_destroy(lbm_case *c) {
     if (!c) return LBM_OK;
+    if (c->batch) batch_forget(c->batch, c);
     DeviceGuard dg(c->p.device);
     cudaFree(c->f);
     cudaFree(c->g);
@@ -573,7 +595,7 @@ int lbm_destroy(lbm_case *c) {
 }
 
 static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, void *stream) {
-    int rc = check_case(c, false);
+    int rc = check_mutable(c, false);
     if (rc) return rc;
     DeviceGuard dg(c->p.device);
     cudaStream_t st = (cudaStream_t)stream;
@@ -609,7 +631,7 @@ int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stre
 int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const double *uy, const double *uz,
                        const double *phi, const double *f, const double *g) {
     (void)rho; (void)ux; (void)uz; (void)phi;
-    int rc = check_case(c, false);
+    int rc = check_mutable(c, false);
     if (rc) return rc;
     if (!uy || !f || !g) return fail(LBM_ERR_ARG, "uy, f and g are required");
     DeviceGuard dg(c->p.device);
@@ -711,7 +733,7 @@ int lbm_store_ref_state(lbm_case *c, double *rho, double *ux, double *uy, double
 }
 
 int lbm_step(lbm_case *c, int32_t nsteps, void *stream) {
-    int rc = check_case(c, true);
+    int rc = check_mutable(c, true);
     if (rc) return rc;
     if (nsteps < 0) return fail(LBM_ERR_ARG, "nsteps < 0");
     DeviceGuard dg(c->p.device);
@@ -751,7 +773,7 @@ int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
         k.dT = c->p.t_hot - c->p.t_cold;
         k.visc = c->d.visc;
         k.step = c->step;
-        obs_finalize<<<1, 32, 0, st>>>(c->partial, c->obs_blocks, k, c->d_obs);
+        obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, c->d_obs);
         return LBM_OK;
     });
     if (rc) return rc;
@@ -842,7 +864,7 @@ int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
 }
 
 int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *stream) {
-    int rc = check_case(c, false);
+    int rc = check_mutable(c, false);
     if (rc) return rc;
     uint64_t of, og, op, pb, cb;
     const uint64_t need = ckpt_layout(c, &of, &og, &op, &pb, &cb);
@@ -945,7 +967,7 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
         k.dT = p->t_hot - p->t_cold;
         k.visc = view.d.visc;
         k.step = step;
-        obs_finalize<<<1, 32, 0, st>>>(scratch, blocks, k, out_dev);
+        obs_finalize<<<1, 32 * kObs, 0, st>>>(scratch, blocks, k, out_dev);
         return LBM_OK;
     });
     view.f = view.g = view.phip = nullptr;
@@ -981,7 +1003,27 @@ int lbm_set_step_kernel(lbm_case *c, int32_t kind) {
     if (kind == LBM_KERNEL_ROW && !row_eligible(c))
         return fail(LBM_ERR_ARG, "the row-staged kernel needs periodic sides, 32 <= LX <= 256 and LX*element "
                                  "size a multiple of 16 bytes");
+    if ((kind == LBM_KERNEL_ROW || kind == LBM_KERNEL_PAIR) && c->collision != LBM_COLLISION_BGK)
+        return fail(LBM_ERR_ARG, "the row-staged and paired kernels collide with BGK only");
     c->kernel = kind;
+    return LBM_OK;
+}
+
+int lbm_set_collision(lbm_case *c, int32_t model) {
+    if (!c) return fail(LBM_ERR_ARG, "case is NULL");
+    if (model != LBM_COLLISION_BGK && model != LBM_COLLISION_REGULARIZED)
+        return fail(LBM_ERR_ARG, "unknown collision model");
+    if (c->batch) return fail(LBM_ERR_STATE, "case is a batch member: remove it from the batch first");
+    if (model != LBM_COLLISION_BGK && (use_row_kernel(c) || use_pair_kernel(c)))
+        return fail(LBM_ERR_ARG, "the regularised collision runs on the node kernel; the case's step kernel is "
+                                 "set to ROW or PAIR");
+    c->collision = model;
+    return LBM_OK;
+}
+
+int lbm_get_collision(const lbm_case *c, int32_t *model) {
+    if (!c || !model) return fail(LBM_ERR_ARG, "NULL argument");
+    *model = c->collision;
     return LBM_OK;
 }
 

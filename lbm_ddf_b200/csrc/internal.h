@@ -19,6 +19,8 @@ struct lbm_case {
     bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
     void *f = nullptr, *g = nullptr, *phip = nullptr;
     int32_t kernel = LBM_KERNEL_AUTO;    // step kernel choice
+    int32_t collision = LBM_COLLISION_BGK;
+    lbm_batch *batch = nullptr;          // the batch the case is a member of
     int *d_err = nullptr;                // set by a step kernel whose bulk-copy wait timed out
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
@@ -33,6 +35,8 @@ size_t store_bytes(int storage);
 int64_t round_up(int64_t v, int64_t m);
 void derive(const lbm_params *p, lbm_derived *d);
 int check_params(const lbm_params *p);
+// drops a case that is being destroyed from its batch (batch.cu)
+void batch_forget(lbm_batch *b, lbm_case *c);
 
 struct DeviceGuard {
     int prev = -1;

@@ -37,6 +37,7 @@
 // same plain bounce-back.
 #pragma once
 
+#include "../../include/lbm_ddf.h"
 #include "lattice.cuh"
 
 namespace lbm {
@@ -77,6 +78,11 @@ template <class S> struct StepArgs {
     // population rows: loads (f, g) and stores (f, g)
     __device__ __forceinline__ S *ld_row(int which, int k) const { return which ? gl[k] : fl[k]; }
     __device__ __forceinline__ S *st_row(int which, int k) const { return which ? gs[k] : fs[k]; }
+    // population k of node j (the accessor interface update_node uses); the
+    // index keeps its type (unsigned node, signed displaced node), which
+    // the register allocation of the update is sensitive to
+    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const { return ld_row(which, k)[j]; }
+    template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const { return st_row(which, k)[j]; }
 };
 
 // Geometry of one node: coordinates, and node-index displacements to the
@@ -140,13 +146,13 @@ __device__ __forceinline__ bool inside_t(const Node &g) {
 }
 
 // Population k (of f when WHICH = 0, of g when 1) of node g at the current
-// time, from either layout.  `a` supplies the row bases: a.ld_row(which, k).
+// time, from either layout.  `a` supplies the addresses: a.ld(which, k, node).
 template <class S, bool SWAPPED, int K, bool INTERIOR = false, int WHICH = 0, class A>
 __device__ __forceinline__ S load_pop(const A &a, const Node &g) {
-    if (!SWAPPED) return a.ld_row(WHICH, K)[g.n];
+    if (!SWAPPED) return a.ld(WHICH, K, g.n);
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
-    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return a.ld_row(WHICH, opp(K))[(int32_t)g.n + disp<DX, DY, DZ>(g)];
-    return a.ld_row(WHICH, K)[g.n];
+    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return a.ld(WHICH, opp(K), (int32_t)g.n + disp<DX, DY, DZ>(g));
+    return a.ld(WHICH, K, g.n);
 }
 
 template <class S, bool SWAPPED, bool INTERIOR = false, class A>
@@ -230,6 +236,96 @@ __device__ __forceinline__ void collide_fast(R (&fr)[Q], R (&gr)[Q], const Momen
     });
 }
 
+// Round-to-nearest operations the compiler never fuses or reorders: code
+// written with them rounds identically in every kernel that inlines it.
+__device__ __forceinline__ float add_rn(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double add_rn(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float sub_rn(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double sub_rn(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float mul_rn(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// Regularised BGK (Latt and Chopard, Math. Comput. Simul. 72 (2006)
+// 165-168), an option beside the reference's BGK for relaxation times near
+// 1/2.  Same equilibria and force term as collide_fast; the non-equilibrium
+// part that relaxes is replaced by its projection on the second-order
+// Hermite polynomial for f and the first-order one for g:
+//   f_i* = feq_i + (1 - 1/tau) 4.5 w_i (c_i c_i : Pi - tr(Pi)/3) + force_i,
+//          Pi = sum_i c_i c_i f_i - (rho/3 I + u u)
+//   g_i* = geq_i + (1 - 1/tau_c) 3 w_i c_i . j,   j = sum_i c_i g_i - phi u
+// (rho/3 I + u u and phi u are the equilibria's own second and first
+// moments on D3Q27).  rho, u and phi are unchanged, as in BGK; at tau = 1 the
+// two models coincide.  Every operation is an explicit round-to-nearest one,
+// so a case gives bitwise the same result in the single-case and the batch
+// kernels, in FP64 and FP32.
+template <class R>
+__device__ __forceinline__ void collide_reg(R (&fr)[Q], R (&gr)[Q], const Moments<R> &m, R omega_f, R omega_g,
+                                            R force_fac, R gb, R t0) {
+    R sxx = 0, syy = 0, szz = 0, sxy = 0, sxz = 0, syz = 0, jx = 0, jy = 0, jz = 0;
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        constexpr int X = cx(K), Y = cy(K), Z = cz(K);
+        const R f = fr[K], g = gr[K];
+        if (X != 0) sxx = add_rn(sxx, f);
+        if (Y != 0) syy = add_rn(syy, f);
+        if (Z != 0) szz = add_rn(szz, f);
+        if (X * Y > 0) sxy = add_rn(sxy, f);
+        if (X * Y < 0) sxy = sub_rn(sxy, f);
+        if (X * Z > 0) sxz = add_rn(sxz, f);
+        if (X * Z < 0) sxz = sub_rn(sxz, f);
+        if (Y * Z > 0) syz = add_rn(syz, f);
+        if (Y * Z < 0) syz = sub_rn(syz, f);
+        if (X > 0) jx = add_rn(jx, g);
+        if (X < 0) jx = sub_rn(jx, g);
+        if (Y > 0) jy = add_rn(jy, g);
+        if (Y < 0) jy = sub_rn(jy, g);
+        if (Z > 0) jz = add_rn(jz, g);
+        if (Z < 0) jz = sub_rn(jz, g);
+    });
+    const R third = R(1) / R(3);
+    const R rho3 = mul_rn(m.rho, third);
+    const R pxx = fma_rn(-m.ux, m.ux, sub_rn(sxx, rho3));
+    const R pyy = fma_rn(-m.uy, m.uy, sub_rn(syy, rho3));
+    const R pzz = fma_rn(-m.uz, m.uz, sub_rn(szz, rho3));
+    const R pxy2 = mul_rn(R(2), fma_rn(-m.ux, m.uy, sxy));
+    const R pxz2 = mul_rn(R(2), fma_rn(-m.ux, m.uz, sxz));
+    const R pyz2 = mul_rn(R(2), fma_rn(-m.uy, m.uz, syz));
+    const R tr3 = mul_rn(add_rn(add_rn(pxx, pyy), pzz), third);
+    jx = fma_rn(-m.phi, m.ux, jx);
+    jy = fma_rn(-m.phi, m.uy, jy);
+    jz = fma_rn(-m.phi, m.uz, jz);
+    const R keep_f = mul_rn(R(4.5), sub_rn(R(1), omega_f)), keep_g = mul_rn(R(3), sub_rn(R(1), omega_g));
+    const R uv = mul_rn(R(3), fma_rn(m.uz, m.uz, fma_rn(m.uy, m.uy, mul_rn(m.ux, m.ux))));
+    const R kf = mul_rn(mul_rn(R(3), force_fac), mul_rn(gb, sub_rn(m.phi, t0)));
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        constexpr int X = cx(K), Y = cy(K), Z = cz(K);
+        constexpr R w = R(wd(K));
+        R cu = R(0), cj = R(0), qpi = -tr3;
+        if (X > 0) { cu = add_rn(cu, m.ux); cj = add_rn(cj, jx); qpi = add_rn(qpi, pxx); }
+        if (X < 0) { cu = sub_rn(cu, m.ux); cj = sub_rn(cj, jx); qpi = add_rn(qpi, pxx); }
+        if (Y > 0) { cu = add_rn(cu, m.uy); cj = add_rn(cj, jy); qpi = add_rn(qpi, pyy); }
+        if (Y < 0) { cu = sub_rn(cu, m.uy); cj = sub_rn(cj, jy); qpi = add_rn(qpi, pyy); }
+        if (Z > 0) { cu = add_rn(cu, m.uz); cj = add_rn(cj, jz); qpi = add_rn(qpi, pzz); }
+        if (Z < 0) { cu = sub_rn(cu, m.uz); cj = sub_rn(cj, jz); qpi = add_rn(qpi, pzz); }
+        if (X * Y > 0) qpi = add_rn(qpi, pxy2);
+        if (X * Y < 0) qpi = sub_rn(qpi, pxy2);
+        if (X * Z > 0) qpi = add_rn(qpi, pxz2);
+        if (X * Z < 0) qpi = sub_rn(qpi, pxz2);
+        if (Y * Z > 0) qpi = add_rn(qpi, pyz2);
+        if (Y * Z < 0) qpi = sub_rn(qpi, pyz2);
+        const R eu = mul_rn(R(3), cu);
+        const R p = add_rn(eu, mul_rn(R(0.5), fma_rn(eu, eu, -uv)));
+        const R feq0 = mul_rn(w, add_rn(R(1), p));
+        const R fneq = mul_rn(mul_rn(keep_f, w), qpi);
+        const R force = mul_rn(mul_rn(kf, sub_rn(R(Y), m.uy)), feq0);
+        fr[K] = add_rn(add_rn(mul_rn(w, add_rn(m.rho, p)), fneq), force);
+        gr[K] = fma_rn(mul_rn(keep_g, w), cj, mul_rn(m.phi, feq0));
+    });
+}
+
 // Correctly rounded a / b for a divisor b known in advance, from its correctly
 // rounded reciprocal y = RN(1/b): q = RN(a y), r = a - b q (exact by FMA),
 // result RN(q + r y).  Markstein's theorem (P. Markstein, IBM J. Res. Dev.
@@ -288,10 +384,12 @@ __device__ __forceinline__ void collide_exact(double (&fr)[Q], double (&gr)[Q], 
     });
 }
 
-template <class S, class A>
+template <class S, int COLL = LBM_COLLISION_BGK, class A>
 __device__ __forceinline__ void collide(typename Codec<S>::R (&fr)[Q], typename Codec<S>::R (&gr)[Q],
                                         const Moments<typename Codec<S>::R> &m, const A &a) {
-    if constexpr (std::is_same<typename Codec<S>::R, double>::value)
+    if constexpr (COLL == LBM_COLLISION_REGULARIZED)
+        collide_reg(fr, gr, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+    else if constexpr (std::is_same<typename Codec<S>::R, double>::value)
         collide_exact(fr, gr, m, a.tau, a.tauc, a.rcp_tau, a.rcp_tauc, a.rcp_rt, a.force_fac, a.gb, a.t0);
     else
         collide_fast(fr, gr, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
@@ -325,24 +423,170 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
             const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
-            a.st_row(0, I)[j] = C::template f_out<I>(fv, a.t0);
-            a.st_row(1, I)[j] = C::template g_out<I>(gv, a.t0);
+            a.st(0, I, j) = C::template f_out<I>(fv, a.t0);
+            a.st(1, I, j) = C::template g_out<I>(gv, a.t0);
         } else {
-            a.st_row(0, opp(I))[g.n] = C::template f_out<I>(fv, a.t0);
-            a.st_row(1, opp(I))[g.n] = C::template g_out<I>(gv, a.t0);
+            a.st(0, opp(I), g.n) = C::template f_out<I>(fv, a.t0);
+            a.st(1, opp(I), g.n) = C::template g_out<I>(gv, a.t0);
         }
     });
 }
 
-// Resident blocks per SM the register allocation is sized for: 4 x 128
-// threads (<= 128 registers) for 4-byte and 2-byte storage, 2 (<= 255) for
-// FP64, which holds 54 doubles across the collision.
-template <class S> struct StepOccupancy { static constexpr int value = sizeof(S) == 8 ? 2 : 4; };
+// Resident 128-thread blocks per SM the register allocation is sized for:
+// 2 (<= 255 registers) for FP64, which holds 54 doubles across the
+// collision; 4 (<= 128) for FP32; LBM_BLOCKS_PER_SM_16 for 16-bit storage,
+// whose update is latency-bound and gains from more resident warps (B200,
+// 256^3 FP16S: 17.5, 19.0 and 19.2 GLUPS at 4, 5 and 6 blocks).
+#ifndef LBM_BLOCKS_PER_SM_16
+#define LBM_BLOCKS_PER_SM_16 6
+#endif
+template <class S> struct StepOccupancy {
+    static constexpr int value = sizeof(S) == 8 ? 2 : sizeof(S) == 4 ? 4 : LBM_BLOCKS_PER_SM_16;
+};
 
 // The whole update of one node: gather, moments, collision, carried
 // temperature, scatter.
+// ---- 16-bit storage: the collision in the stored, normalised variables ----
+//
+// FP16S / BF16S rows hold fh_i = f_i / w_i and gh_i = g_i / w_i - t0.  The
+// update below works on those directly (FP32 arithmetic): the moments sum
+// them per weight class and weight the four class sums, and the BGK steps in
+// normalised form,
+//   fh*_i = fh_i - (fh_i - (rho + p_i)) / tau + 3 (1 - 1/(2 tau)) F_y (c_iy - u_y) (1 + p_i)
+//   gh*_i = gh_i - (gh_i + t0 - phi (1 + p_i)) / tau_c,
+// p_i = 3 c_i.u + 4.5 (c_i.u)^2 - 1.5 u^2, need no weight on load or store.
+// Opposite directions share c.u and the quadratic part of p.  The same
+// update as collide_fast, with fewer instructions per node.
+template <class S> __device__ __forceinline__ float h2f(S s);
+template <> __device__ __forceinline__ float h2f<__half>(__half s) { return __half2float(s); }
+template <> __device__ __forceinline__ float h2f<__nv_bfloat16>(__nv_bfloat16 s) { return __bfloat162float(s); }
+template <class S> __device__ __forceinline__ S f2h(float v);
+template <> __device__ __forceinline__ __half f2h<__half>(float v) { return __float2half_rn(v); }
+template <> __device__ __forceinline__ __nv_bfloat16 f2h<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
+
+template <class S, bool SWAPPED, bool INTERIOR, class A>
+__device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        fh[K] = h2f<S>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g));
+        gh[K] = h2f<S>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g));
+    });
+}
+
+__device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], const float (&gh)[Q], float phip,
+                                                       float gbeta, float t0) {
+    float r[4] = {0.f, 0.f, 0.f, 0.f}, x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f},
+          z[4] = {0.f, 0.f, 0.f, 0.f}, t[4] = {0.f, 0.f, 0.f, 0.f};
+    Unroll<0, Q>::run([&](auto kk) {
+        constexpr int K = decltype(kk)::value;
+        constexpr int C = wclass(K);
+        r[C] += fh[K];
+        if (cx(K) > 0) x[C] += fh[K];
+        if (cx(K) < 0) x[C] -= fh[K];
+        if (cy(K) > 0) y[C] += fh[K];
+        if (cy(K) < 0) y[C] -= fh[K];
+        if (cz(K) > 0) z[C] += fh[K];
+        if (cz(K) < 0) z[C] -= fh[K];
+        t[C] += gh[K];
+    });
+    const float w0 = (float)wd(0), w1 = (float)wd(1), w2 = (float)wd(7), w3 = (float)wd(19);
+    Moments<float> m;
+    m.rho = fmaf(w3, r[3], fmaf(w2, r[2], fmaf(w1, r[1], w0 * r[0])));
+    m.ux = fmaf(w3, x[3], fmaf(w2, x[2], w1 * x[1]));
+    const float jy = fmaf(w3, y[3], fmaf(w2, y[2], w1 * y[1]));
+    m.uz = fmaf(w3, z[3], fmaf(w2, z[2], w1 * z[1]));
+    m.phi = fmaf(w3, t[3], fmaf(w2, t[2], fmaf(w1, t[1], w0 * t[0]))) + t0;   // sum w_i (gh_i + t0)
+    m.uy = jy + 0.5f * (gbeta * (phip - t0));
+    return m;
+}
+
+// Both relaxations as affine maps of the old value, with per-node
+// coefficients (k = kf (c_y - u_y) takes three values, one per c_y):
+//   fh* = (1 - om_f) fh + (om_f rho + k) + (om_f + k) p
+//   gh* = (1 - om_g) gh + om_g (phi - t0) + om_g phi p
+// and p_I, p_J = (q +/- 2 eu) / 2 with q = eu^2 - 3 u^2 for a pair of
+// opposite directions: two multiply-adds per population and three per pair.
+__device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
+                                             float om_g, float force_fac, float gbeta, float t0) {
+    const float ux3 = 3.f * m.ux, uy3 = 3.f * m.uy, uz3 = 3.f * m.uz;
+    const float uv = 3.f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
+    const float kf = 3.f * force_fac * (gbeta * (m.phi - t0));
+    const float k_m = kf * (-1.f - m.uy), k_0 = kf * (-m.uy), k_p = kf * (1.f - m.uy);
+    const float af = 1.f - om_f, orho = om_f * m.rho;
+    const float c0[3] = {orho + k_m, orho + k_0, orho + k_p};    // indexed by c_y + 1
+    const float c1[3] = {om_f + k_m, om_f + k_0, om_f + k_p};
+    const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - t0);
+    auto relax = [&](float &f, float &g, float p, int cy1) {
+        f = fmaf(af, f, fmaf(c1[cy1], p, c0[cy1]));
+        g = fmaf(ag, g, fmaf(d1, p, d0));
+    };
+    relax(fh[0], gh[0], -0.5f * uv, 1);
+    Unroll<1, Q>::run([&](auto ii) {
+        constexpr int I = decltype(ii)::value;
+        constexpr int J = opp(I);
+        if constexpr (I < J) {
+            float eu = 0.f;
+            if (cx(I) > 0) eu += ux3;
+            if (cx(I) < 0) eu -= ux3;
+            if (cy(I) > 0) eu += uy3;
+            if (cy(I) < 0) eu -= uy3;
+            if (cz(I) > 0) eu += uz3;
+            if (cz(I) < 0) eu -= uz3;
+            const float q = fmaf(eu, eu, -uv);
+            relax(fh[I], gh[I], fmaf(0.5f, q, eu), cy(I) + 1);
+            relax(fh[J], gh[J], fmaf(0.5f, q, -eu), cy(J) + 1);
+        }
+    });
+}
+
+// scatter() for the normalised variables: anti-bounce-back in normalised
+// form, gh' = 2 T_wall (1 + rho) - gh* - 2 t0, and no weights on store.
+template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
+__device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float (&fh)[Q], const float (&gh)[Q],
+                                             float rho) {
+    Unroll<0, Q>::run([&](auto ii) {
+        constexpr int I = decltype(ii)::value;
+        constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
+        float gv = gh[I];
+        const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
+        const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * a.t0;
+        if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
+            const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
+            a.st(0, I, j) = f2h<S>(fh[I]);
+            a.st(1, I, j) = f2h<S>(gv);
+        } else {
+            a.st(0, opp(I), g.n) = f2h<S>(fh[I]);
+            a.st(1, opp(I), g.n) = f2h<S>(gv);
+        }
+    });
+}
+
 template <class S, bool SWAPPED, bool PERIODIC, class A>
+__device__ __forceinline__ void update_node_norm(const A &a, uint32_t n) {
+    const Node g = make_node<PERIODIC>(a, n);
+    float fh[Q], gh[Q];
+    const bool interior = PERIODIC && g.vym && g.vyp;
+    if (interior)
+        gather_norm<S, SWAPPED, true>(a, g, fh, gh);
+    else
+        gather_norm<S, SWAPPED, false>(a, g, fh, gh);
+    Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0);
+    if (a.use_phi_fix) m.phi = a.phi_fix;
+    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+    a.phip[n] = m.phi;
+    if (interior)
+        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho);
+    else
+        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho);
+}
+
+template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A>
 __device__ __forceinline__ void update_node(const A &a, uint32_t n) {
+    if constexpr (sizeof(S) == 2 && COLL == LBM_COLLISION_BGK) {
+        update_node_norm<S, SWAPPED, PERIODIC>(a, n);
+        return;
+    }
     using R = typename Codec<S>::R;
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
@@ -354,7 +598,7 @@ __device__ __forceinline__ void update_node(const A &a, uint32_t n) {
     else
         gather<S, SWAPPED, false>(a, g, fr, gr);
     const Moments<R> m = node_moments<S>(a, fr, gr, n);
-    collide<S>(fr, gr, m, a);
+    collide<S, COLL>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
     if (interior)
         scatter<S, SWAPPED, PERIODIC, true>(a, g, fr, gr, m.rho);
@@ -362,11 +606,11 @@ __device__ __forceinline__ void update_node(const A &a, uint32_t n) {
         scatter<S, SWAPPED, PERIODIC, false>(a, g, fr, gr, m.rho);
 }
 
-template <class S, bool SWAPPED, bool PERIODIC>
+template <class S, bool SWAPPED, bool PERIODIC, int COLL>
 __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.nodes) return;
-    update_node<S, SWAPPED, PERIODIC>(a, n);
+    update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
 }
 
 }  // namespace lbm

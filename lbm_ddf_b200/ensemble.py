@@ -51,6 +51,7 @@ def _case(spec, storage, device, stream=None):
     p = make_params(spec["lx"], spec["ly"], spec["lz"], rayleigh=spec["rayleigh"], prandtl=spec["prandtl"],
                     sides=SIDES_PERIODIC, storage=storage, device=device)
     c = Case(p)
+    c.set_collision(spec.get("collision", "bgk"))
     c.init_conduction(spec["seed"], 1e-3, stream=stream)
     return c
 
@@ -171,11 +172,15 @@ def main(argv=None) -> int:
     ap.add_argument("--baseline-cases", type=int, default=0, help="run the baseline on the first N cases (0: all)")
     ap.add_argument("--last-steps", type=int, default=2000, help="time average of Nu over the last steps")
     ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--collision", default="bgk", choices=["bgk", "regularized"],
+                    help="collision model of every case, in every run")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
     specs = ensemble_specs(args.cases, args.seed)
+    for sp in specs:
+        sp["collision"] = args.collision
     report = {"config": {"cases": args.cases, "steps": args.steps, "obs_every": args.obs_every, "seed": args.seed,
-                         "grids": GRIDS, "ra": [1e4, 1e7], "pr": PRANDTL}}
+                         "grids": GRIDS, "ra": [1e4, 1e7], "pr": PRANDTL, "collision": args.collision}}
     runs = {}
     for st in [x for x in args.storage.split(",") if x]:
         runs[st] = run_batched(specs, st, args.steps, args.obs_every)

@@ -45,6 +45,7 @@ class Request:
     steps: int
     storage: str
     seed: int
+    collision: str = "bgk"         # or "regularized"
 
     def params(self, device=0):
         return make_params(self.lx, self.ly, self.lz, rayleigh=self.rayleigh, prandtl=self.prandtl,
@@ -135,6 +136,7 @@ class Server:
         if self.used + need > self.budget or len(self.resident) >= self.max_members:
             return False
         c = Case(r.params(self.device))
+        c.set_collision(r.collision)
         c.init_conduction(r.seed, 1e-3, stream=self.stream)
         self._batch(r.storage).add(c)
         self.used += need
@@ -226,6 +228,7 @@ def fp64_rerun(r: Request, obs_every: int, device: int = 0) -> list:
                     storage="f64", device=device)
     series = []
     with Case(p) as c:
+        c.set_collision(r.collision)
         c.init_conduction(r.seed, 1e-3)
         while c.step_count < r.steps:
             c.step(obs_every)
@@ -246,10 +249,14 @@ def main(argv=None) -> int:
     ap.add_argument("--sample-fp64", type=int, default=10, help="completed cases rerun in FP64 for the Nu error")
     ap.add_argument("--last-fraction", type=float, default=0.4, help="Nu time average over this last fraction")
     ap.add_argument("--seed", type=int, default=7)
+    ap.add_argument("--collision", default="bgk", choices=["bgk", "regularized"],
+                    help="collision model of every request (the FP64 reruns use the same)")
     ap.add_argument("--out", default=None)
     args = ap.parse_args(argv)
 
     reqs = make_requests(args.requests, args.seed, step_scale=args.step_scale, obs_every=args.obs_every)
+    for r in reqs:
+        r.collision = args.collision
     rate = calibrate()
     demand = np.mean([r.nodes * r.steps / rate[r.storage] for r in reqs])   # GPU-seconds per request
     arrivals_per_s = args.utilisation / demand
@@ -260,7 +267,8 @@ def main(argv=None) -> int:
     done = [x for x in res if not x.diverged]
     report = {
         "config": {"requests": args.requests, "step_scale": args.step_scale, "utilisation": args.utilisation,
-                   "budget_gb": args.budget_gb, "obs_every": args.obs_every, "seed": args.seed},
+                   "budget_gb": args.budget_gb, "obs_every": args.obs_every, "seed": args.seed,
+                   "collision": args.collision},
         "calibrated_node_steps_per_s": rate,
         "mean_demand_gpu_s": float(demand), "arrival_rate_per_s": float(arrivals_per_s),
         "elapsed_s": srv.elapsed, "busy_s": srv.busy_seconds,

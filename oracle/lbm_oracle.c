@@ -65,6 +65,7 @@ struct orc_state {
     double *rho, *ux, *uy, *uz, *phi, *fx, *fy, *fz;
     double w[ORC_Q];
     int opp[ORC_Q];
+    int collision;          /* ORC_COLLISION_BGK (the reference) or _REGULARIZED */
 };
 
 /* Lattice weights, src/initial.cu:77-83. */
@@ -229,6 +230,84 @@ static void k_collide_g(orc_state *s) {
     }
 }
 
+/* Regularised BGK, an engine option the reference does not have (Latt and
+ * Chopard, Math. Comput. Simul. 72 (2006) 165-168).  The equilibria and the
+ * force term are those of k_collide_f / k_collide_g; only the relaxed
+ * non-equilibrium part changes.  For f it is replaced by its projection on
+ * the second-order Hermite polynomial,
+ *   fneq_i -> w_i / (2 cs^4) (c_i c_i - cs^2 I) : Pi,  cs^2 = 1/3,
+ *   Pi = sum_i c_i c_i (f_i - feq_i) = sum_i c_i c_i f_i - (rho/3 I + u u)
+ * (the second moment of this feq is rho/3 I + u u on D3Q27), so
+ *   f_i <- feq_i + (1 - 1/tau) fneq_i + force_i.
+ * For g it is replaced by its first-order projection,
+ *   gneq_i -> w_i c_i . j / cs^2,  j = sum_i c_i g_i - phi u,
+ *   g_i <- geq_i + (1 - 1/tau_c) gneq_i.
+ * Mass, momentum and phi are those of BGK; at tau = 1 both are feq + force. */
+static void k_collide_f_reg(orc_state *s) {
+    const double tau = s->p.tau;
+    const double keep = 1.0 - 1.0 / tau, force_fac = 1.0 - 0.5 / tau;
+    const int64_t n = s->n;
+    double *f = s->f;
+#pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < n; idx++) {
+        const double fy = s->fy[idx], rho = s->rho[idx];
+        const double u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
+        const double uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        double m2[3][3] = {{0}};
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            const int c[3] = {CX[ip], CY[ip], CZ[ip]};
+            const double fi = f[ip * n + idx];
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) m2[a][b] += (double)(c[a] * c[b]) * fi;
+        }
+        double pi[3][3];
+        for (int a = 0; a < 3; a++)
+            for (int b = 0; b < 3; b++) pi[a][b] = m2[a][b] - (a == b ? rho / 3.0 : 0.0) - u[a] * u[b];
+        const double tr3 = (pi[0][0] + pi[1][1] + pi[2][2]) / 3.0;
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            const int c[3] = {CX[ip], CY[ip], CZ[ip]};
+            const double eu = 3.0 * (c[0] * u[0] + c[1] * u[1] + c[2] * u[2]);
+            const double p = eu + 0.5 * (eu * eu - uv);
+            const double feq = s->w[ip] * (rho + p);
+            const double feq0 = s->w[ip] * (1.0 + p);
+            double qpi = -tr3;
+            for (int a = 0; a < 3; a++)
+                for (int b = 0; b < 3; b++) qpi += (double)(c[a] * c[b]) * pi[a][b];
+            const double fneq = 4.5 * s->w[ip] * qpi;
+            const double fc = force_fac * fy * ((double)c[1] - u[1]) * 3.0;
+            f[ip * n + idx] = feq + keep * fneq + fc * feq0;
+        }
+    }
+}
+
+static void k_collide_g_reg(orc_state *s) {
+    const double keep = 1.0 - 1.0 / s->p.tauc;
+    const int64_t n = s->n;
+    double *g = s->g;
+#pragma omp parallel for schedule(static)
+    for (int64_t idx = 0; idx < n; idx++) {
+        const double phi = s->phi[idx];
+        const double u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
+        const double uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        double j[3] = {-phi * u[0], -phi * u[1], -phi * u[2]};
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            const double gi = g[ip * n + idx];
+            j[0] += (double)CX[ip] * gi;
+            j[1] += (double)CY[ip] * gi;
+            j[2] += (double)CZ[ip] * gi;
+        }
+        for (int ip = 0; ip < ORC_Q; ip++) {
+            const double eu = 3.0 * (CX[ip] * u[0] + CY[ip] * u[1] + CZ[ip] * u[2]);
+            const double geq = s->w[ip] * phi * (1.0 + eu + 0.5 * (eu * eu - uv));
+            const double gneq = 3.0 * s->w[ip] * (CX[ip] * j[0] + CY[ip] * j[1] + CZ[ip] * j[2]);
+            g[ip * n + idx] = geq + keep * gneq;
+        }
+    }
+}
+
+void orc_set_collision(orc_state *s, int model) { s->collision = model; }
+int orc_get_collision(const orc_state *s) { return s->collision; }
+
 /* Pull streaming with wall rules, src/streaming.cu:3-125 (scalar = 0, field f)
  * and :127-251 (scalar = 1, field g).
  *
@@ -310,8 +389,13 @@ void orc_step(orc_state *s, int nsteps) {
     size_t bytes = (size_t)ORC_Q * (size_t)s->n * sizeof(double);
     for (int it = 0; it < nsteps; it++) {
         k_forcing(s);          /* src/main.cu:27 */
-        k_collide_f(s);        /* :29 */
-        k_collide_g(s);        /* :33 */
+        if (s->collision == ORC_COLLISION_REGULARIZED) {
+            k_collide_f_reg(s);
+            k_collide_g_reg(s);
+        } else {
+            k_collide_f(s);    /* :29 */
+            k_collide_g(s);    /* :33 */
+        }
         k_stream(s, 0);        /* :38 */
         memcpy(s->f, s->f_temp, bytes);   /* :39 */
         k_stream(s, 1);        /* :40 */

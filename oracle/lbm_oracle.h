@@ -98,6 +98,14 @@ void orc_observables(const orc_state *s, double out[10]);
  * <ux>, <uy>, <uz>, <phi>, phi_rms, written to out[5*iy + k]. */
 void orc_profile(const orc_state *s, double *out);
 
+/* Collision model: ORC_COLLISION_BGK (default) is the reference's; the
+ * regularised BGK of Latt and Chopard (2006) is an engine option the
+ * reference does not have (see lbm_oracle.c k_collide_f_reg). */
+#define ORC_COLLISION_BGK 0
+#define ORC_COLLISION_REGULARIZED 1
+void orc_set_collision(orc_state *s, int model);
+int orc_get_collision(const orc_state *s);
+
 /* Contraction model (see lbm_oracle.c): 1 = round as the nvcc-built
  * reference does (default), 0 = every operation rounded separately. */
 void orc_set_contract(int on);

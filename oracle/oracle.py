@@ -75,6 +75,8 @@ def lib():
         L.orc_profile.argtypes = [C.c_void_p, dp]
         L.orc_threads.restype = C.c_int
         L.orc_set_contract.argtypes = [C.c_int]
+        L.orc_set_collision.argtypes = [C.c_void_p, C.c_int]
+        L.orc_get_collision.argtypes = [C.c_void_p]
         L.orc_get_contract.restype = C.c_int
         _lib = L
     return _lib
@@ -101,6 +103,9 @@ def make_params(lx, ly, lz, rayleigh=1e5, prandtl=0.71, t_hot=1.0, t_cold=0.0,
     if lib().orc_derive(C.byref(p)) != 0:
         raise ValueError("bad grid for the oracle")
     return p
+
+
+COLLISIONS = {"bgk": 0, "regularized": 1}
 
 
 class Oracle:
@@ -147,6 +152,15 @@ class Oracle:
 
     def step(self, n: int = 1):
         lib().orc_step(self._h, int(n))
+
+    def set_collision(self, model: str):
+        """'bgk' (the reference's) or 'regularized' (Latt and Chopard 2006)."""
+        lib().orc_set_collision(self._h, COLLISIONS[model])
+
+    @property
+    def collision(self) -> str:
+        code = lib().orc_get_collision(self._h)
+        return next(k for k, v in COLLISIONS.items() if v == code)
 
     def observables(self) -> dict:
         out = np.zeros(10)

@@ -31,7 +31,7 @@ def test_exports_every_declared_symbol(lbm):
 
 
 def test_abi_version(lbm):
-    assert lbm.lib().lbm_abi_version() == 1
+    assert lbm.lib().lbm_abi_version() == 2
 
 
 def test_derive_matches_reference_globals(lbm, oracle_mod):

@@ -179,6 +179,61 @@ def test_init_then_step_on_another_stream(lbm, oracle_mod):
             assert np.array_equal(c.store_ref_state(("f",))["f"], want), rep
 
 
+@pytest.mark.parametrize("storage", ["f64", "f16s"])
+def test_mixed_collision_models(lbm, storage):
+    """Members with BGK and regularised collision in one batch: each equals
+    the same case stepped alone (FP64 bitwise; the regularised update is
+    written with explicit rounding, so its 16-bit members are bitwise too)."""
+    models = ["regularized", "bgk", "regularized", "bgk"]
+    solo = make_cases(lbm, storage)
+    for c, m in zip(solo, models):
+        c.set_collision(m)
+        c.step(6)
+    want = states(solo)
+    cases = make_cases(lbm, storage)
+    for c, m in zip(cases, models):
+        c.set_collision(m)
+    with lbm.Batch(storage) as b:
+        for c in cases:
+            b.add(c)
+        b.step(6)
+        got = states(cases)
+    for m, x, y in zip(models, want, got):
+        for k in x:
+            if storage == "f64" or m == "regularized":
+                assert np.array_equal(x[k], y[k]), (m, k)
+            else:
+                assert relerr(y[k], x[k]) <= 2e-3, k
+    for c in solo + cases:
+        c.close()
+
+
+def test_member_rules(lbm):
+    """A case belongs to one batch; calls that change a member's state are
+    refused until it leaves; destroying a member removes it."""
+    cases = make_cases(lbm, "f32", MIX[:3])
+    with lbm.Batch("f32") as a, lbm.Batch("f32") as b:
+        for c in cases:
+            a.add(c)
+        with pytest.raises(lbm.LbmError):
+            b.add(cases[0])                  # already in another batch
+        for call in (lambda c: c.step(1), lambda c: c.init_conduction(1), lambda c: c.set_collision("bgk")):
+            with pytest.raises(lbm.LbmError) as e:
+                call(cases[1])
+            assert e.value.code == lbm.ERR_STATE
+        cases[1].observables()               # reading is fine
+        cases[2].close()                     # destroying a member removes it
+        assert a.size()[0] == 2
+        a.step(2)
+        a.remove(cases[1])
+        cases[1].step(1)
+        b.add(cases[1])
+        b.step(1)
+        assert cases[0].step_count == 2 and cases[1].step_count == 4
+    for c in cases[:2]:
+        c.close()
+
+
 def test_batch_rejections(lbm):
     with lbm.Batch("f32") as b:
         with lbm.Case(lbm.make_params(16, 8, 8, sides=lbm.SIDES_WALL, storage="f32")) as w:

@@ -251,16 +251,15 @@ def test_row_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
 def test_pair_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
     """Two nodes per thread (16-bit storage): same results as the node
     kernel, on rows whose pairs fill whole warps and on rows where warps
-    straddle rows (x-shift realigned across lanes and at row ends)."""
+    straddle rows (x-shift realigned across lanes and at row ends).  The node
+    kernel collides 16-bit data in normalised variables, the paired one in
+    weighted ones: same mathematics, FP32 rounding apart."""
     p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage)
     a, oa = _run_kind(lbm, p, 6, lbm.KERNEL_NODE)
     b, ob = _run_kind(lbm, p, 6, lbm.KERNEL_PAIR)
     tol = {"f16s": 2e-3, "bf16s": 2e-2}[storage]
     for k in ("f", "g", "phi"):
         assert relerr(b[k], a[k]) <= tol, k
-    # nearly every stored value agrees bit for bit (the two kernels may fuse
-    # FP32 multiply-adds differently, flipping a rare 16-bit rounding)
-    assert np.mean(a["f"] == b["f"]) > 0.95
 
 
 def test_pair_kernel_eligibility(lbm):
@@ -316,6 +315,74 @@ def test_reduced_precision_vs_oracle(lbm, oracle_mod, storage, tol, steps, perio
     compare(got, o, 20 * tol, fields=("uy",))
     ob = o.observables()
     assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= 50 * tol
+
+
+# ---------------------------------------------------------------- regularised collision
+
+@pytest.mark.parametrize("storage,tol,steps", [("f64", 1e-12, 200), ("f32", 5e-5, 200), ("f16s", 5e-3, 100),
+                                               ("bf16s", 4e-2, 100)])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_regularized_vs_oracle(lbm, oracle_mod, storage, tol, steps, periodic):
+    """LBM_COLLISION_REGULARIZED against the oracle's restatement of the same
+    model: FP64 to 1e-12 (the two compilers fuse multiply-adds differently),
+    reduced storage to the tolerances of the BGK path."""
+    lx, ly, lz = 24, 20, 16
+    o = oracle_mod.Oracle(oracle_mod.make_params(lx, ly, lz, rayleigh=1e6, prandtl=0.71, periodic_sides=periodic))
+    o.set_collision("regularized")
+    o.init_conduction(21, 1e-2)
+    o.step(steps)
+    p = lbm.make_params(lx, ly, lz, rayleigh=1e6, prandtl=0.71, storage=storage,
+                        sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL)
+    with lbm.Case(p) as c:
+        assert c.collision == "bgk"
+        c.set_collision("regularized")
+        assert c.collision == "regularized"
+        c.init_conduction(21, 1e-2)
+        c.step(steps)
+        got = c.store_ref_state()
+        got["obs"] = c.observables()
+    compare(got, o, tol, fields=("f", "g", "phi"))
+    compare(got, o, 1e-12 if storage == "f64" else 20 * tol, fields=("uy",))
+    ob = o.observables()
+    assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= (1e-10 if storage == "f64" else 50 * tol)
+
+
+def test_regularized_stays_stable_where_bgk_diverges(lbm):
+    """An under-resolved case, 32 x 16 x 32 at Ra 1e8, Pr 4.38 (tau_f =
+    0.5010, tau_g = 0.5002): BGK blows up within a few thousand steps, the
+    regularised collision stays finite and convecting (on B200 BGK diverged
+    by step 2500 and the regularised model ran 30000 steps)."""
+    p = lbm.make_params(32, 16, 32, rayleigh=1e8, prandtl=4.38, sides=lbm.SIDES_PERIODIC, storage="f32")
+    res = {}
+    for model in ("bgk", "regularized"):
+        with lbm.Case(p) as c:
+            c.set_collision(model)
+            c.init_conduction(11, 1e-3)
+            c.step(6000)
+            res[model] = c.observables(allow_diverged=True)
+    assert res["bgk"]["diverged"] == 1
+    assert res["regularized"]["diverged"] == 0 and res["regularized"]["nu_bulk"] > 2.0
+
+
+def test_collision_model_rules(lbm):
+    p = lbm.make_params(32, 12, 16, sides=lbm.SIDES_PERIODIC, storage="f32")
+    with lbm.Case(p) as c:
+        with pytest.raises(lbm.LbmError):
+            c.set_collision(7)
+        c.set_collision("regularized")
+        with pytest.raises(lbm.LbmError):
+            c.set_step_kernel(lbm.KERNEL_ROW)          # the row kernel collides with BGK only
+        c.set_collision("bgk")
+        c.set_step_kernel(lbm.KERNEL_ROW)
+        with pytest.raises(lbm.LbmError):
+            c.set_collision("regularized")
+        c.set_step_kernel(lbm.KERNEL_AUTO)
+        c.set_collision("regularized")
+        c.init_conduction(3)
+        c.step(4)                                        # regularised steps, then BGK ones
+        c.set_collision("bgk")
+        c.step(4)
+        assert c.step_count == 8
 
 
 # ---------------------------------------------------------------- failure detection

@@ -28,6 +28,19 @@ def small_requests(lbm):
     return reqs
 
 
+class TickClock:
+    """A clock that advances 10 ms per reading: the server's schedule (which
+    arrivals meet which running chunks) is then the same on every GPU,
+    however fast the chunks run."""
+
+    def __init__(self):
+        self.t = 0.0
+
+    def __call__(self):
+        self.t += 0.01
+        return self.t
+
+
 def test_server_completes_under_budget_and_alone_equals_mix(lbm):
     from lbm_ddf_b200.serve import Request, Server
 
@@ -35,7 +48,7 @@ def test_server_completes_under_budget_and_alone_equals_mix(lbm):
     need = [lbm.case_bytes(r.params()) for r in reqs]
     budget = 2.5 * max(need)                            # at most two or three resident at once
     srv = Server(budget_bytes=budget, obs_every=100)
-    res = srv.run(reqs)
+    res = srv.run(reqs, clock=TickClock())
     assert srv.peak_used <= budget
     assert srv.peak_resident >= 2                       # work did overlap
     for r, x in zip(reqs, res):
@@ -43,6 +56,8 @@ def test_server_completes_under_budget_and_alone_equals_mix(lbm):
         assert x.steps == r.steps
         assert len(x.series) == r.steps // 100
         assert x.finished >= x.admitted >= r.arrival
+    # some request joined while an earlier one was still running
+    assert any(0 < b.admitted < a.finished and a.admitted < b.admitted for a in res for b in res)
     # each result alone
     for k in (0, 5):
         r = reqs[k]
