@@ -195,11 +195,10 @@ def run_engine(args):
     stream = torch.cuda.Stream(device=dev)
     bytes_per_lu = 2 * 27 * 2 * lbm.STORAGE_BYTES[p.storage]
 
-    kind = {"auto": lbm.KERNEL_AUTO, "node": lbm.KERNEL_NODE, "row": lbm.KERNEL_ROW,
-            "pair": lbm.KERNEL_PAIR}[args.kernel]
+    kind = {"auto": lbm.KERNEL_AUTO, "node": lbm.KERNEL_NODE, "row": lbm.KERNEL_ROW}[args.kernel]
     case = lbm.Case(p)
     case.set_step_kernel(kind)
-    kernel_used = {lbm.KERNEL_NODE: "node", lbm.KERNEL_ROW: "row", lbm.KERNEL_PAIR: "pair"}[case.step_kernel]
+    kernel_used = {lbm.KERNEL_NODE: "node", lbm.KERNEL_ROW: "row"}[case.step_kernel]
     case.init_conduction(1000 + rank, 1e-3, stream=stream)
     case.step(args.warmup, stream=stream)
     torch.cuda.synchronize()
@@ -242,7 +241,7 @@ def run_engine(args):
         p64 = lbm.make_params(w["lx"], w["ly"], w["lz"], rayleigh=w["rayleigh"], prandtl=w["prandtl"],
                               sides=lbm.SIDES_PERIODIC, storage="f64", device=dev)
         c64 = lbm.Case(p64)
-        c64.set_step_kernel(kind if kind != lbm.KERNEL_PAIR else lbm.KERNEL_AUTO)
+        c64.set_step_kernel(kind)
         c64.init_conduction(1000 + rank, 1e-3, stream=stream)
         c64.step(args.warmup, stream=stream)
         barrier(world)
@@ -364,7 +363,7 @@ def main(argv=None):
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--grid", type=int, default=256)
     ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s"])
-    ap.add_argument("--kernel", default="auto", choices=["auto", "node", "row", "pair"])
+    ap.add_argument("--kernel", default="auto", choices=["auto", "node", "row"])
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-f64", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=15.0)

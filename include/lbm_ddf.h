@@ -54,16 +54,15 @@ extern "C" {
 /* population storage in HBM; arithmetic is FP64 for F64 and FP32 otherwise */
 #define LBM_STORE_F64 0
 #define LBM_STORE_F32 1
-#define LBM_STORE_F16S 2       /* FP16 of f_i/w_i and g_i/w_i - t0 */
-#define LBM_STORE_BF16S 3      /* BF16 of the same shifted values */
+#define LBM_STORE_F16S 2       /* FP16 of f_i/w_i and g_i/w_i - t0, stored as (f, g) pairs */
+#define LBM_STORE_BF16S 3      /* BF16 of the same shifted values, stored as (f, g) pairs */
 
 /* step kernels (same results, different data movement) */
 #define LBM_KERNEL_AUTO 0      /* NODE (measured the fastest on B200) */
 #define LBM_KERNEL_NODE 1      /* one node per thread, any grid and side-wall mode */
-#define LBM_KERNEL_ROW 2       /* whole x-rows staged by bulk copies; periodic sides,
-                                  32 <= LX <= 256, LX*element size a multiple of 16 bytes */
-#define LBM_KERNEL_PAIR 3      /* two nodes per thread, 32-bit accesses; 16-bit storage,
-                                  periodic sides, even LX */
+#define LBM_KERNEL_ROW 2       /* whole x-rows staged by bulk copies; FP32 or FP64 storage,
+                                  periodic sides, 32 <= LX <= 256, LX*element size a
+                                  multiple of 16 bytes */
 
 /* collision models */
 #define LBM_COLLISION_BGK 0          /* the reference's BGK (src/collision.cu:3-88); default */
@@ -186,7 +185,10 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
  *   f, g      27 population rows each, row k at base + k*pop_stride elements,
  *             in p->storage's format and in the layout `swapped` names
  *             (0 natural, 1 swapped; a case's layout is swapped after an odd
- *             number of steps from an init or load);
+ *             number of steps from an init or load).  For F16S / BF16S the
+ *             engine interleaves the two: one array of (f, g) pairs, row k
+ *             at f + 2*k*pop_stride elements, node j's f at element 2j and
+ *             its g at 2j + 1; pass g = f + 1 element;
  *   phi_prev  previous-step temperature per node (double for F64, else float);
  *   out_dev   DEVICE memory for one lbm_observables, written on `stream`.
  * Enqueues two kernels on `stream` and returns without synchronising; the
@@ -221,7 +223,7 @@ int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
 /* Chooses the collision model of a case (LBM_COLLISION_*; BGK at creation),
  * in effect from its next step.  The regularised model runs on the node
  * kernel (and in batches); LBM_ERR_ARG if the case's step kernel is set to
- * ROW or PAIR.  No counterpart in the reference, which has BGK only. */
+ * ROW.  No counterpart in the reference, which has BGK only. */
 int lbm_set_collision(lbm_case *c, int32_t model);
 int lbm_get_collision(const lbm_case *c, int32_t *model);
 

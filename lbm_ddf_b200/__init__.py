@@ -30,7 +30,7 @@ SIDES_WALL, SIDES_PERIODIC = 0, 1
 STORE_F64, STORE_F32, STORE_F16S, STORE_BF16S = 0, 1, 2, 3
 STORAGE_NAMES = {"f64": STORE_F64, "f32": STORE_F32, "f16s": STORE_F16S, "bf16s": STORE_BF16S}
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32: 4, STORE_F16S: 2, STORE_BF16S: 2}
-KERNEL_AUTO, KERNEL_NODE, KERNEL_ROW, KERNEL_PAIR = 0, 1, 2, 3
+KERNEL_AUTO, KERNEL_NODE, KERNEL_ROW = 0, 1, 2
 COLLISION_BGK, COLLISION_REGULARIZED = 0, 1
 COLLISION_NAMES = {"bgk": COLLISION_BGK, "regularized": COLLISION_REGULARIZED}
 

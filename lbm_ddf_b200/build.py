@@ -22,7 +22,7 @@ DRIVER = os.path.join(PKG, "rb3d")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
 LIB_SOURCES = ["engine.cu", "batch.cu"]
-HEADERS = ["lattice.cuh", "step.cuh", "bulk.cuh", "rowstep.cuh", "pair16.cuh", "internal.h"]
+HEADERS = ["lattice.cuh", "step.cuh", "bulk.cuh", "rowstep.cuh", "internal.h"]
 
 
 def _newer(target: str, deps: list[str]) -> bool:

@@ -53,23 +53,31 @@ template <class S> struct BatchCase {
     R omega_f, omega_g, force_fac, gb, t0, t_hot, t_cold, phi_fix;
     int32_t use_phi_fix, pad;
 
-    // element k * ps + j of the population array, indexed in 32 bits (a
-    // member has 27 ps < 2^32 elements per array): one multiply-add per
-    // access and no 64-bit row addresses held in registers
+    // element (k * ps + j) * elem_stride of the population array, indexed
+    // in 32 bits (a member has 27 ps elem_stride < 2^32 elements per
+    // array): one multiply-add per access and no 64-bit row addresses held
+    // in registers
     template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const {
-        return (which ? g : f)[(uint32_t)k * ps + (uint32_t)j];
+        return (which ? g : f)[((uint32_t)k * ps + (uint32_t)j) * elem_stride<S>()];
     }
     template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const {
-        return (which ? g_st : f_st)[(uint32_t)k * ps + (uint32_t)j];
+        return (which ? g_st : f_st)[((uint32_t)k * ps + (uint32_t)j) * elem_stride<S>()];
+    }
+    // 16-bit storage: the (f_k, g_k) pair of node j as one 32-bit word
+    template <class I, class SS = S> __device__ __forceinline__ typename Pack16<SS>::T ld2(int k, I j) const {
+        return reinterpret_cast<const typename Pack16<SS>::T *>(f)[(uint32_t)k * ps + (uint32_t)j];
+    }
+    template <class I, class SS = S> __device__ __forceinline__ typename Pack16<SS>::T &st2(int k, I j) const {
+        return reinterpret_cast<typename Pack16<SS>::T *>(f_st)[(uint32_t)k * ps + (uint32_t)j];
     }
 };
 
 // Resident threads per SM the batch kernel's registers are sized for: those
-// of the single-case kernel, except 640 for 16-bit storage (96 registers: the
-// members' parameters come from a descriptor in memory rather than from the
-// constant bank, and the swapped-layout update spills at 80).
+// of the single-case kernel, except 512 (128 registers) for 16-bit storage:
+// one 256^3 FP16S case through the batch kernel on B200 ran at 15.7 GLUPS
+// with 640 threads (96 registers) and 19.2-20.9 with 512.
 template <class S> constexpr int batch_threads_per_sm() {
-    return sizeof(S) == 2 ? 640 : StepOccupancy<S>::value * 128;
+    return sizeof(S) == 2 ? 512 : StepOccupancy<S>::value * 128;
 }
 template <class S, int BLOCK> struct BatchOccupancy {
     static constexpr int value = batch_threads_per_sm<S>() / BLOCK > 0 ? batch_threads_per_sm<S>() / BLOCK : 1;
@@ -349,8 +357,9 @@ int lbm_batch_add(lbm_batch *b, lbm_case *c) {
     if (c->p.sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "batches run periodic-side cases only");
     if (c->rest_phi) return fail(LBM_ERR_STATE, "take the first step of a rest-state case alone before batching it");
     if (c->batch) return fail(LBM_ERR_ARG, c->batch == b ? "case is already in the batch" : "case is in another batch");
-    if ((uint64_t)Q * (uint64_t)c->ps >= (1ull << 32))
-        return fail(LBM_ERR_ARG, "case too large for a batch (27 x padded nodes must stay below 2^32)");
+    if ((uint64_t)Q * (uint64_t)c->ps * (interleaved(c) ? 2u : 1u) >= (1ull << 32))
+        return fail(LBM_ERR_ARG, "case too large for a batch (its population array must have fewer than 2^32 "
+                                 "elements)");
     if ((int)b->members.size() >= kMaxBatch) return fail(LBM_ERR_ARG, "batch is full");
     b->members.push_back(c);
     c->batch = b;

@@ -21,7 +21,6 @@
 #include <vector>
 
 #include "internal.h"
-#include "pair16.cuh"
 #include "rowstep.cuh"
 #include "step.cuh"
 
@@ -259,9 +258,9 @@ __global__ void import_pop_kernel(const StepArgs<S> a, int which, int k, const d
         if (K == k) {
             using R = typename C::R;
             if (which)
-                a.gs[K][n] = C::template g_out<K>((R)v, a.t0);
+                a.st(1, K, n) = C::template g_out<K>((R)v, a.t0);
             else
-                a.fs[K][n] = C::template f_out<K>((R)v, a.t0);
+                a.st(0, K, n) = C::template f_out<K>((R)v, a.t0);
         }
     });
 }
@@ -304,8 +303,8 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         const double gk = __dmul_rn(wd(K), t);
-        a.fs[K][n] = C::template f_out<K>((R)0, a.t0);
-        a.gs[K][n] = C::template g_out<K>((R)gk, a.t0);
+        a.st(0, K, n) = C::template f_out<K>((R)0, a.t0);
+        a.st(1, K, n) = C::template g_out<K>((R)gk, a.t0);
     });
     a.phip[n] = (typename C::P)t;
 }
@@ -343,6 +342,9 @@ int check_params(const lbm_params *p) {
     if (nodes > 2147483647.0) return fail(LBM_ERR_ARG, "more than 2^31-1 nodes in one case");
     if (p->sides != LBM_SIDES_WALL && p->sides != LBM_SIDES_PERIODIC) return fail(LBM_ERR_ARG, "bad sides");
     if (store_bytes(p->storage) == 0) return fail(LBM_ERR_ARG, "bad storage");
+    // 16-bit pair rows are addressed with 32-bit indices below 9 padded rows
+    if (store_bytes(p->storage) == 2 && 9.0 * (double)round_up((int64_t)nodes, 128) >= 4294967296.0)
+        return fail(LBM_ERR_ARG, "16-bit storage holds at most 477,218,560 nodes per case (FP32 beyond)");
     if (!(p->rayleigh > 0) || !(p->prandtl > 0)) return fail(LBM_ERR_ARG, "Ra and Pr must be positive");
     if (!(p->t_hot > p->t_cold)) return fail(LBM_ERR_ARG, "T_hot must exceed T_cold");
     if (!(p->gravity * p->beta > 0)) return fail(LBM_ERR_ARG, "gravity*beta must be positive");
@@ -372,9 +374,12 @@ template <class S> StepArgs<S> make_args(const lbm_case *c) {
     using R = typename Codec<S>::R;
     StepArgs<S> a;
     for (int k = 0; k < Q; k++) {
-        a.fl[k] = a.fs[k] = (S *)c->f + (size_t)k * (size_t)c->ps;
-        a.gl[k] = a.gs[k] = (S *)c->g + (size_t)k * (size_t)c->ps;
+        a.fl[k] = a.fs[k] = (S *)c->f + (size_t)k * (size_t)c->ps * elem_stride<S>();
+        a.gl[k] = a.gs[k] = (S *)c->g + (size_t)k * (size_t)c->ps * elem_stride<S>();
     }
+    for (int b = 0; b < 3; b++)
+        a.pairs[b] = a.pairs_st[b] = (S *)c->f + (size_t)(9 * b) * (size_t)c->ps * elem_stride<S>();
+    a.pair_row = (uint32_t)c->ps;
     a.phip = (typename Codec<S>::P *)c->phip;
     a.lx = c->p.lx;
     a.ly = c->p.ly;
@@ -420,25 +425,20 @@ template <class S, bool SW, bool PER> void launch_step_t(const lbm_case *c, cons
         step_kernel<S, SW, PER, LBM_COLLISION_BGK><<<grid, kStepThreads, 0, st>>>(a);
 }
 
-// Whether the row-staged kernel (rowstep.cuh) can run this case.
+// Whether the row-staged kernel (rowstep.cuh) can run this case: periodic
+// sides, rows of 32-256 nodes whose bytes are a multiple of 16, FP32 or FP64
+// storage (16-bit storage interleaves f and g, which the row staging does
+// not handle; its node kernel already moves both in one 32-bit access).
 bool row_eligible(const lbm_case *c) {
     const size_t sb = store_bytes(c->p.storage);
-    return c->p.sides == LBM_SIDES_PERIODIC && c->p.lx >= 32 && c->p.lx <= 256 && ((size_t)c->p.lx * sb) % 16 == 0;
-}
-
-// Whether the paired-node 16-bit kernel (pair16.cuh) can run this case.
-bool pair_eligible(const lbm_case *c) {
-    return (c->p.storage == LBM_STORE_F16S || c->p.storage == LBM_STORE_BF16S) &&
-           c->p.sides == LBM_SIDES_PERIODIC && (c->p.lx % 2) == 0;
+    return !interleaved(c) && c->p.sides == LBM_SIDES_PERIODIC && c->p.lx >= 32 && c->p.lx <= 256 &&
+           ((size_t)c->p.lx * sb) % 16 == 0;
 }
 
 // LBM_KERNEL_AUTO runs the node kernel: on B200 it measured faster than the
-// row-staged kernel (whose bulk copies do not raise the bandwidth the node
-// kernel already reaches) and, for 16-bit storage, than the paired kernel
-// (13.7 against 17.0 GLUPS at 256^3: fewer, wider accesses, but two
-// collisions per thread at 168 registers leave too few warps to hide latency).
+// row-staged kernel, whose bulk copies do not raise the bandwidth the node
+// kernel already reaches.
 bool use_row_kernel(const lbm_case *c) { return c->kernel == LBM_KERNEL_ROW; }
-bool use_pair_kernel(const lbm_case *c) { return c->kernel == LBM_KERNEL_PAIR; }
 
 template <class S, bool SW, int PITCH>
 cudaError_t launch_row_p(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
@@ -460,23 +460,13 @@ template <class S, bool SW> cudaError_t launch_row_t(const lbm_case *c, const St
     return launch_row_p<S, SW, 256>(c, a, st);
 }
 
-template <class S> void launch_pair(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
-    if constexpr (sizeof(S) == 2) {
-        const int64_t pairs = c->nodes / 2;
-        if (c->swapped) pair16_kernel<S, true><<<grid_for(pairs, 128), 128, 0, st>>>(a);
-        else pair16_kernel<S, false><<<grid_for(pairs, 128), 128, 0, st>>>(a);
-    }
-}
-
 template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
-    if (use_pair_kernel(c)) {
-        launch_pair<S>(c, a, st);
-        return;
-    }
-    if (use_row_kernel(c)) {
-        if (c->swapped) launch_row_t<S, true>(c, a, st);
-        else launch_row_t<S, false>(c, a, st);
-        return;
+    if constexpr (elem_stride<S>() == 1) {
+        if (use_row_kernel(c)) {
+            if (c->swapped) launch_row_t<S, true>(c, a, st);
+            else launch_row_t<S, false>(c, a, st);
+            return;
+        }
     }
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
@@ -563,8 +553,14 @@ int lbm_create(const lbm_params *p, lbm_case **out) {
     const size_t sb = store_bytes(p->storage);
     const size_t pop_bytes = (size_t)Q * (size_t)c->ps * sb;
     const size_t carry_bytes = (size_t)c->ps * (p->storage == LBM_STORE_F64 ? 8 : 4);
-    cudaError_t e = cudaMalloc(&c->f, pop_bytes);
-    if (e == cudaSuccess) e = cudaMalloc(&c->g, pop_bytes);
+    cudaError_t e;
+    if (interleaved(c)) {   // one array of (f, g) pairs; g starts one element in
+        e = cudaMalloc(&c->f, 2 * pop_bytes);
+        if (e == cudaSuccess) c->g = (char *)c->f + sb;
+    } else {
+        e = cudaMalloc(&c->f, pop_bytes);
+        if (e == cudaSuccess) e = cudaMalloc(&c->g, pop_bytes);
+    }
     if (e == cudaSuccess) e = cudaMalloc(&c->phip, carry_bytes);
     if (e == cudaSuccess) e = cudaMalloc(&c->partial, (size_t)c->obs_blocks * kObs * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&c->d_obs, sizeof(lbm_observables));
@@ -585,7 +581,7 @@ int lbm_destroy(lbm_case *c) {
     if (c->batch) batch_forget(c->batch, c);
     DeviceGuard dg(c->p.device);
     cudaFree(c->f);
-    cudaFree(c->g);
+    if (!interleaved(c)) cudaFree(c->g);
     cudaFree(c->phip);
     cudaFree(c->partial);
     cudaFree(c->d_obs);
@@ -813,7 +809,7 @@ int lbm_get_profile(lbm_case *c, double *out, void *stream) {
 
 // Checkpoint image: header, f, g, phip (each region 256-byte aligned).
 struct CheckpointHeader {
-    char magic[8];          // "LBMDDF1\0"
+    char magic[8];          // "LBMDDF2\0" (16-bit states hold interleaved (f, g) pairs)
     lbm_params p;
     int64_t step;
     int32_t swapped;
@@ -848,7 +844,7 @@ int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
     DeviceGuard dg(c->p.device);
     CheckpointHeader h;
     std::memset(&h, 0, sizeof h);
-    std::memcpy(h.magic, "LBMDDF1", 8);
+    std::memcpy(h.magic, "LBMDDF2", 8);
     h.p = c->p;
     h.step = c->step;
     h.swapped = c->swapped ? 1 : 0;
@@ -857,8 +853,12 @@ int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
     std::memcpy(host, &h, sizeof h);
     cudaStream_t st = (cudaStream_t)stream;
     char *b = (char *)host;
-    CUDA_TRY(cudaMemcpyAsync(b + of, c->f, pb, cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(b + og, c->g, pb, cudaMemcpyDeviceToHost, st));
+    if (interleaved(c)) {   // the f and g regions are one array of pairs
+        CUDA_TRY(cudaMemcpyAsync(b + of, c->f, 2 * pb, cudaMemcpyDeviceToHost, st));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(b + of, c->f, pb, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(b + og, c->g, pb, cudaMemcpyDeviceToHost, st));
+    }
     CUDA_TRY(cudaMemcpyAsync(b + op, c->phip, cb, cudaMemcpyDeviceToHost, st));
     return LBM_OK;
 }
@@ -871,7 +871,7 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
     if (!host || bytes < need) return fail(LBM_ERR_ARG, "checkpoint buffer missing or too small");
     CheckpointHeader h;
     std::memcpy(&h, host, sizeof h);
-    if (std::memcmp(h.magic, "LBMDDF1", 8) != 0) return fail(LBM_ERR_ARG, "not an engine checkpoint");
+    if (std::memcmp(h.magic, "LBMDDF2", 8) != 0) return fail(LBM_ERR_ARG, "not an engine checkpoint");
     if (h.p.lx != c->p.lx || h.p.ly != c->p.ly || h.p.lz != c->p.lz || h.p.storage != c->p.storage ||
         h.p.sides != c->p.sides || h.ps != c->ps || h.p.rayleigh != c->p.rayleigh || h.p.prandtl != c->p.prandtl ||
         h.p.beta != c->p.beta || h.p.gravity != c->p.gravity || h.p.t_hot != c->p.t_hot || h.p.t_cold != c->p.t_cold)
@@ -879,8 +879,12 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
     DeviceGuard dg(c->p.device);
     cudaStream_t st = (cudaStream_t)stream;
     const char *b = (const char *)host;
-    CUDA_TRY(cudaMemcpyAsync(c->f, b + of, pb, cudaMemcpyHostToDevice, st));
-    CUDA_TRY(cudaMemcpyAsync(c->g, b + og, pb, cudaMemcpyHostToDevice, st));
+    if (interleaved(c)) {
+        CUDA_TRY(cudaMemcpyAsync(c->f, b + of, 2 * pb, cudaMemcpyHostToDevice, st));
+    } else {
+        CUDA_TRY(cudaMemcpyAsync(c->f, b + of, pb, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(c->g, b + og, pb, cudaMemcpyHostToDevice, st));
+    }
     CUDA_TRY(cudaMemcpyAsync(c->phip, b + op, cb, cudaMemcpyHostToDevice, st));
     c->step = h.step;
     c->swapped = h.swapped != 0;
@@ -996,15 +1000,13 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
 
 int lbm_set_step_kernel(lbm_case *c, int32_t kind) {
     if (!c) return fail(LBM_ERR_ARG, "case is NULL");
-    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_NODE && kind != LBM_KERNEL_ROW && kind != LBM_KERNEL_PAIR)
+    if (kind != LBM_KERNEL_AUTO && kind != LBM_KERNEL_NODE && kind != LBM_KERNEL_ROW)
         return fail(LBM_ERR_ARG, "unknown step kernel");
-    if (kind == LBM_KERNEL_PAIR && !pair_eligible(c))
-        return fail(LBM_ERR_ARG, "the paired kernel needs 16-bit storage, periodic sides and an even LX");
     if (kind == LBM_KERNEL_ROW && !row_eligible(c))
-        return fail(LBM_ERR_ARG, "the row-staged kernel needs periodic sides, 32 <= LX <= 256 and LX*element "
-                                 "size a multiple of 16 bytes");
-    if ((kind == LBM_KERNEL_ROW || kind == LBM_KERNEL_PAIR) && c->collision != LBM_COLLISION_BGK)
-        return fail(LBM_ERR_ARG, "the row-staged and paired kernels collide with BGK only");
+        return fail(LBM_ERR_ARG, "the row-staged kernel needs FP32 or FP64 storage, periodic sides, "
+                                 "32 <= LX <= 256 and LX*element size a multiple of 16 bytes");
+    if (kind == LBM_KERNEL_ROW && c->collision != LBM_COLLISION_BGK)
+        return fail(LBM_ERR_ARG, "the row-staged kernel collides with BGK only");
     c->kernel = kind;
     return LBM_OK;
 }
@@ -1014,9 +1016,9 @@ int lbm_set_collision(lbm_case *c, int32_t model) {
     if (model != LBM_COLLISION_BGK && model != LBM_COLLISION_REGULARIZED)
         return fail(LBM_ERR_ARG, "unknown collision model");
     if (c->batch) return fail(LBM_ERR_STATE, "case is a batch member: remove it from the batch first");
-    if (model != LBM_COLLISION_BGK && (use_row_kernel(c) || use_pair_kernel(c)))
+    if (model != LBM_COLLISION_BGK && use_row_kernel(c))
         return fail(LBM_ERR_ARG, "the regularised collision runs on the node kernel; the case's step kernel is "
-                                 "set to ROW or PAIR");
+                                 "set to ROW");
     c->collision = model;
     return LBM_OK;
 }
@@ -1029,7 +1031,7 @@ int lbm_get_collision(const lbm_case *c, int32_t *model) {
 
 int lbm_get_step_kernel(const lbm_case *c, int32_t *kind) {
     if (!c || !kind) return fail(LBM_ERR_ARG, "NULL argument");
-    *kind = use_pair_kernel(c) ? LBM_KERNEL_PAIR : use_row_kernel(c) ? LBM_KERNEL_ROW : LBM_KERNEL_NODE;
+    *kind = use_row_kernel(c) ? LBM_KERNEL_ROW : LBM_KERNEL_NODE;
     return LBM_OK;
 }
 

@@ -17,6 +17,8 @@ struct lbm_case {
     bool swapped = false;
     bool initialised = false;
     bool rest_phi = false;               // next step uses phi = 0.5 (reference rest state)
+    // f and g: separate arrays of 27 rows (FP64, FP32), or for 16-bit
+    // storage one array of (f, g) pairs with g = f + one element
     void *f = nullptr, *g = nullptr, *phip = nullptr;
     int32_t kernel = LBM_KERNEL_AUTO;    // step kernel choice
     int32_t collision = LBM_COLLISION_BGK;
@@ -28,6 +30,11 @@ struct lbm_case {
 };
 
 namespace lbm_internal {
+
+// 16-bit storage keeps f and g interleaved (lattice.cuh elem_stride)
+inline bool interleaved(const lbm_case *c) {
+    return c->p.storage == LBM_STORE_F16S || c->p.storage == LBM_STORE_BF16S;
+}
 
 // records `msg` for lbm_last_error() on this thread and returns `code`
 int fail(int code, const std::string &msg);

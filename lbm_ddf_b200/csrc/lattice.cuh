@@ -107,6 +107,25 @@ template <> struct Codec<__nv_bfloat16> {
     template <int I> __device__ __forceinline__ static __nv_bfloat16 g_out(R v, R t0) { return __float2bfloat16_rn(fmaf(v, (float)winv(I), -t0)); }
 };
 
+// 16-bit storage interleaves the two distributions: element 2j of row k is
+// f_k at node j and element 2j + 1 is g_k there, so one 32-bit access moves
+// both (f_k and g_k always travel to the same slot of the same node).  FP32
+// and FP64 keep separate f and g arrays.
+template <class S> __host__ __device__ constexpr int elem_stride() { return sizeof(S) == 2 ? 2 : 1; }
+
+// the packed (f_k, g_k) pair of 16-bit storage and its conversions
+template <class S> struct Pack16;
+template <> struct Pack16<__half> {
+    using T = __half2;
+    __device__ __forceinline__ static float2 unpack(T v) { return __half22float2(v); }
+    __device__ __forceinline__ static T pack(float f, float g) { return __floats2half2_rn(f, g); }
+};
+template <> struct Pack16<__nv_bfloat16> {
+    using T = __nv_bfloat162;
+    __device__ __forceinline__ static float2 unpack(T v) { return __bfloat1622float2(v); }
+    __device__ __forceinline__ static T pack(float f, float g) { return __floats2bfloat162_rn(f, g); }
+};
+
 // compile-time loop: calls fn(std::integral_constant<int, I>) for I = 0..N-1
 template <int I, int N> struct Unroll {
     template <class Fn> __device__ __forceinline__ static void run(Fn &&fn) {

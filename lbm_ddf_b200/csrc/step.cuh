@@ -45,10 +45,11 @@ namespace lbm {
 template <class S> struct StepArgs {
     using R = typename Codec<S>::R;
     using P = typename Codec<S>::P;
-    // Base address of each population row (row k of f at fl[k]).  Kernel
-    // parameters live in the constant bank, so an access costs one
-    // multiply-add of a 32-bit node index onto a constant, whatever the
-    // case's size.
+    // Base address of each population row (row k of f at fl[k]; for 16-bit
+    // storage the rows hold (f, g) pairs and gl[k] = fl[k] + 1 element, see
+    // elem_stride).  Kernel parameters live in the constant bank, so an
+    // access costs one multiply-add of a 32-bit node index onto a constant,
+    // whatever the case's size.
     S *fl[Q];
     S *gl[Q];
     // The same addresses again, used only for the stores.  In the
@@ -81,8 +82,32 @@ template <class S> struct StepArgs {
     // population k of node j (the accessor interface update_node uses); the
     // index keeps its type (unsigned node, signed displaced node), which
     // the register allocation of the update is sensitive to
-    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const { return ld_row(which, k)[j]; }
-    template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const { return st_row(which, k)[j]; }
+    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const {
+        if constexpr (elem_stride<S>() == 1) return ld_row(which, k)[j];
+        else return ld_row(which, k)[2u * (uint32_t)j];
+    }
+    template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const {
+        if constexpr (elem_stride<S>() == 1) return st_row(which, k)[j];
+        else return st_row(which, k)[2u * (uint32_t)j];
+    }
+    // 16-bit storage: the (f_k, g_k) pair of node j as one 32-bit word.
+    // The pair array is addressed in three blocks of nine rows, pair
+    // (k mod 9) * pair_row + j of block k / 9, with a 32-bit index (one
+    // multiply-add and one wide add per access; on B200 this ran 18% faster
+    // than the per-row bases above, which FP32 and FP64 keep: for them the
+    // same indexing measured within 1%).  The index stays below
+    // 9 pair_row < 2^32 for every case the C ABI accepts in 16-bit storage.
+    template <class I, class SS = S> __device__ __forceinline__ typename Pack16<SS>::T ld2(int k, I j) const {
+        return reinterpret_cast<const typename Pack16<SS>::T *>(pairs[k / 9])[(uint32_t)(k % 9) * pair_row +
+                                                                              (uint32_t)j];
+    }
+    template <class I, class SS = S> __device__ __forceinline__ typename Pack16<SS>::T &st2(int k, I j) const {
+        return reinterpret_cast<typename Pack16<SS>::T *>(pairs_st[k / 9])[(uint32_t)(k % 9) * pair_row +
+                                                                           (uint32_t)j];
+    }
+    S *pairs[3];       // 16-bit storage: rows 0, 9 and 18 of the (f, g) pair array
+    S *pairs_st[3];    // the same, for the stores (see fs)
+    uint32_t pair_row; // pairs per row (the padded node count)
 };
 
 // Geometry of one node: coordinates, and node-index displacements to the
@@ -155,14 +180,30 @@ __device__ __forceinline__ S load_pop(const A &a, const Node &g) {
     return a.ld(WHICH, K, g.n);
 }
 
+// The (f_k, g_k) pair that node g collides in this step, as load_pop finds
+// each value, with one 32-bit load.
+template <class S, bool SWAPPED, int K, bool INTERIOR, class A>
+__device__ __forceinline__ typename Pack16<S>::T load_pair(const A &a, const Node &g) {
+    if (!SWAPPED) return a.ld2(K, g.n);
+    constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
+    if (inside_t<INTERIOR, DX, DY, DZ>(g)) return a.ld2(opp(K), (int32_t)g.n + disp<DX, DY, DZ>(g));
+    return a.ld2(K, g.n);
+}
+
 template <class S, bool SWAPPED, bool INTERIOR = false, class A>
 __device__ __forceinline__ void gather(const A &a, const Node &g, typename Codec<S>::R (&fr)[Q],
                                        typename Codec<S>::R (&gr)[Q]) {
     using C = Codec<S>;
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g), a.t0);
-        gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g), a.t0);
+        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: Codec's f_in / g_in on the unpacked values
+            const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
+            fr[K] = (float)wd(K) * v.x;
+            gr[K] = (float)wd(K) * (v.y + a.t0);
+        } else {
+            fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g), a.t0);
+            gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g), a.t0);
+        }
     });
 }
 
@@ -421,7 +462,13 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
-        if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
+        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: Codec's f_out / g_out, packed
+            const auto v = Pack16<S>::pack(fv * (float)winv(I), fmaf(gv, (float)winv(I), -a.t0));
+            if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
+                a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
+            else
+                a.st2(opp(I), g.n) = v;
+        } else if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
             const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
             a.st(0, I, j) = C::template f_out<I>(fv, a.t0);
             a.st(1, I, j) = C::template g_out<I>(gv, a.t0);
@@ -434,21 +481,19 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
 
 // Resident 128-thread blocks per SM the register allocation is sized for:
 // 2 (<= 255 registers) for FP64, which holds 54 doubles across the
-// collision; 4 (<= 128) for FP32; LBM_BLOCKS_PER_SM_16 for 16-bit storage,
-// whose update is latency-bound and gains from more resident warps (B200,
-// 256^3 FP16S: 17.5, 19.0 and 19.2 GLUPS at 4, 5 and 6 blocks).
-#ifndef LBM_BLOCKS_PER_SM_16
-#define LBM_BLOCKS_PER_SM_16 6
-#endif
+// collision; 4 (<= 128) for FP32 and 16-bit storage (B200, 256^3 FP16S with
+// interleaved pairs: 21.7 GLUPS at 4 blocks, 14.2 at 5 and 14.6 at 6, where
+// the update spills).
 template <class S> struct StepOccupancy {
-    static constexpr int value = sizeof(S) == 8 ? 2 : sizeof(S) == 4 ? 4 : LBM_BLOCKS_PER_SM_16;
+    static constexpr int value = sizeof(S) == 8 ? 2 : 4;
 };
 
 // The whole update of one node: gather, moments, collision, carried
 // temperature, scatter.
 // ---- 16-bit storage: the collision in the stored, normalised variables ----
 //
-// FP16S / BF16S rows hold fh_i = f_i / w_i and gh_i = g_i / w_i - t0.  The
+// FP16S / BF16S rows hold (fh_i, gh_i) pairs, fh_i = f_i / w_i and
+// gh_i = g_i / w_i - t0, one 32-bit word per population and node.  The
 // update below works on those directly (FP32 arithmetic): the moments sum
 // them per weight class and weight the four class sums, and the BGK steps in
 // normalised form,
@@ -457,19 +502,14 @@ template <class S> struct StepOccupancy {
 // p_i = 3 c_i.u + 4.5 (c_i.u)^2 - 1.5 u^2, need no weight on load or store.
 // Opposite directions share c.u and the quadratic part of p.  The same
 // update as collide_fast, with fewer instructions per node.
-template <class S> __device__ __forceinline__ float h2f(S s);
-template <> __device__ __forceinline__ float h2f<__half>(__half s) { return __half2float(s); }
-template <> __device__ __forceinline__ float h2f<__nv_bfloat16>(__nv_bfloat16 s) { return __bfloat162float(s); }
-template <class S> __device__ __forceinline__ S f2h(float v);
-template <> __device__ __forceinline__ __half f2h<__half>(float v) { return __float2half_rn(v); }
-template <> __device__ __forceinline__ __nv_bfloat16 f2h<__nv_bfloat16>(float v) { return __float2bfloat16_rn(v); }
 
 template <class S, bool SWAPPED, bool INTERIOR, class A>
 __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        fh[K] = h2f<S>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g));
-        gh[K] = h2f<S>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g));
+        const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
+        fh[K] = v.x;
+        gh[K] = v.y;
     });
 }
 
@@ -540,7 +580,8 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
 }
 
 // scatter() for the normalised variables: anti-bounce-back in normalised
-// form, gh' = 2 T_wall (1 + rho) - gh* - 2 t0, and no weights on store.
+// form, gh' = 2 T_wall (1 + rho) - gh* - 2 t0, no weights on store, and one
+// 32-bit store of the packed (f, g) pair per population.
 template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
 __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float (&fh)[Q], const float (&gh)[Q],
                                              float rho) {
@@ -551,14 +592,11 @@ __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const fl
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * a.t0;
-        if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g)) {
-            const int32_t j = (int32_t)g.n + disp<DX, DY, DZ>(g);
-            a.st(0, I, j) = f2h<S>(fh[I]);
-            a.st(1, I, j) = f2h<S>(gv);
-        } else {
-            a.st(0, opp(I), g.n) = f2h<S>(fh[I]);
-            a.st(1, opp(I), g.n) = f2h<S>(gv);
-        }
+        const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
+        if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
+            a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
+        else
+            a.st2(opp(I), g.n) = v;
     });
 }
 

@@ -195,8 +195,9 @@ class Server:
         return [results[r.rid] for r in reqs]
 
 
-def calibrate(storages=("f16s", "f32"), device=0, steps=200) -> dict:
-    """Node-steps per second of a batch of typical cases, per storage."""
+def calibrate(storages=("f16s", "f32"), device=0, steps=200, collision="bgk") -> dict:
+    """Node-steps per second of a batch of typical cases, per storage, with
+    the collision model the requests use."""
     import torch
 
     torch.cuda.set_device(device)
@@ -207,6 +208,7 @@ def calibrate(storages=("f16s", "f32"), device=0, steps=200) -> dict:
         with Batch(STORAGE_NAMES[st], device) as b:
             for r in reqs:
                 c = Case(r.params(device))
+                c.set_collision(collision)
                 c.init_conduction(r.seed, 1e-3)
                 b.add(c)
                 cases.append(c)
@@ -257,7 +259,7 @@ def main(argv=None) -> int:
     reqs = make_requests(args.requests, args.seed, step_scale=args.step_scale, obs_every=args.obs_every)
     for r in reqs:
         r.collision = args.collision
-    rate = calibrate()
+    rate = calibrate(collision=args.collision)
     demand = np.mean([r.nodes * r.steps / rate[r.storage] for r in reqs])   # GPU-seconds per request
     arrivals_per_s = args.utilisation / demand
     assign_arrivals(reqs, arrivals_per_s, seed=args.seed + 1)

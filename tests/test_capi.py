@@ -34,6 +34,12 @@ def test_abi_version(lbm):
     assert lbm.lib().lbm_abi_version() == 2
 
 
+def test_largest_16bit_case_accepted(lbm):
+    """512 x 512 x 1024 in FP16S (268 M nodes) is within the pair index range."""
+    p = lbm.make_params(512, 512, 1024, storage="f16s")
+    assert lbm.lib().lbm_derive(C.byref(p), C.byref(lbm.LbmDerived())) == lbm.OK
+
+
 def test_derive_matches_reference_globals(lbm, oracle_mod):
     """src/globals.cu:13-23, via the oracle's restatement."""
     for (lx, ly, lz, ra, pr) in [(64, 64, 64, 1e5, 0.71), (256, 256, 256, 1e7, 0.71), (512, 256, 512, 1e8, 4.38)]:
@@ -57,6 +63,7 @@ def test_reference_default_beta(lbm):
 @pytest.mark.parametrize("bad", [
     dict(lx=1), dict(ly=2), dict(lz=0), dict(sides=7), dict(storage=9), dict(rayleigh=-1.0),
     dict(prandtl=0.0), dict(t_hot=0.0), dict(gravity=0.0),
+    dict(lx=800, ly=800, lz=800, storage=2),   # 16-bit pair rows beyond 32-bit indexing
 ])
 def test_bad_params_rejected(lbm, bad):
     p = lbm.make_params(8, 8, 8)

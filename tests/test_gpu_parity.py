@@ -229,16 +229,14 @@ def _run_kind(lbm, p, steps, kind, seed=9):
         return c.store_ref_state(("f", "g", "uy", "phi")), c.observables()
 
 
-@pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "bf16s"])
+@pytest.mark.parametrize("storage", ["f64", "f32"])
 @pytest.mark.parametrize("lx,ly,lz", [(32, 12, 10), (48, 10, 16), (64, 9, 8)])
 def test_row_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
-    """Same update, different data movement: FP64 bitwise, FP32 to rounding,
-    16-bit storage to a few storage ulps (FP32 fusion choices can differ
-    between the two kernels and flip a 16-bit rounding)."""
+    """Same update, different data movement: FP64 bitwise, FP32 to rounding."""
     p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage)
     a, oa = _run_kind(lbm, p, 5, lbm.KERNEL_NODE)
     b, ob = _run_kind(lbm, p, 5, lbm.KERNEL_ROW)
-    tol = {"f64": 0.0, "f32": 1e-6, "f16s": 2e-3, "bf16s": 2e-2}[storage]
+    tol = {"f64": 0.0, "f32": 1e-6}[storage]
     for k in ("f", "g", "phi"):
         if tol == 0.0:
             assert np.array_equal(a[k], b[k]), k
@@ -246,33 +244,32 @@ def test_row_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
             assert relerr(b[k], a[k]) <= tol, k
 
 
-@pytest.mark.parametrize("storage", ["f16s", "bf16s"])
-@pytest.mark.parametrize("lx,ly,lz", [(64, 12, 10), (48, 10, 16), (34, 9, 8), (6, 7, 5), (2, 5, 4)])
-def test_pair_kernel_matches_node_kernel(lbm, storage, lx, ly, lz):
-    """Two nodes per thread (16-bit storage): same results as the node
-    kernel, on rows whose pairs fill whole warps and on rows where warps
-    straddle rows (x-shift realigned across lanes and at row ends).  The node
-    kernel collides 16-bit data in normalised variables, the paired one in
-    weighted ones: same mathematics, FP32 rounding apart."""
-    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage)
-    a, oa = _run_kind(lbm, p, 6, lbm.KERNEL_NODE)
-    b, ob = _run_kind(lbm, p, 6, lbm.KERNEL_PAIR)
-    tol = {"f16s": 2e-3, "bf16s": 2e-2}[storage]
-    for k in ("f", "g", "phi"):
-        assert relerr(b[k], a[k]) <= tol, k
+@pytest.mark.parametrize("storage,tol", [("f16s", 5e-3), ("bf16s", 4e-2)])
+@pytest.mark.parametrize("lx,ly,lz,periodic", [(33, 9, 8, True), (6, 7, 5, True), (2, 5, 4, True), (5, 6, 3, False)])
+def test_interleaved_16bit_small_and_odd_grids(lbm, oracle_mod, storage, tol, lx, ly, lz, periodic):
+    """16-bit states are (f, g) pairs moved by 32-bit accesses: grids whose
+    rows do not fill warps, odd LX and two-node rows against the oracle."""
+    steps = 40
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage=storage)
+    got = engine_run(lbm, p, steps, seed=17, amplitude=1e-2)
+    o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=17, amplitude=1e-2)
+    compare(got, o, tol, fields=("f", "g", "phi"))
+    # a checkpoint of the pair array restores the same state
+    with lbm.Case(p) as c:
+        c.init_conduction(17, 1e-2)
+        c.step(steps)
+        import torch
 
-
-def test_pair_kernel_eligibility(lbm):
-    with lbm.Case(lbm.make_params(32, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f16s")) as c:
-        assert c.step_kernel == lbm.KERNEL_NODE          # the default
-        c.set_step_kernel(lbm.KERNEL_PAIR)
-        assert c.step_kernel == lbm.KERNEL_PAIR
-    with lbm.Case(lbm.make_params(33, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f16s")) as c:
-        assert c.step_kernel == lbm.KERNEL_NODE          # odd LX
-        with pytest.raises(lbm.LbmError):
-            c.set_step_kernel(lbm.KERNEL_PAIR)
-    with lbm.Case(lbm.make_params(32, 8, 8, sides=lbm.SIDES_WALL, storage="bf16s")) as c:
-        assert c.step_kernel == lbm.KERNEL_NODE          # closed box
+        buf = bytearray(c.checkpoint_bytes())
+        c.save_state(buf)
+        torch.cuda.synchronize()
+        with lbm.Case(p) as d:
+            d.restore_state(buf)
+            d.step(3)
+            c.step(3)
+            a, b = c.store_ref_state(("f", "g")), d.store_ref_state(("f", "g"))
+    for k in a:
+        assert np.array_equal(a[k], b[k]), k
 
 
 @pytest.mark.parametrize("steps", [1, 2, 7])
@@ -298,6 +295,9 @@ def test_row_kernel_eligibility(lbm):
         assert c.step_kernel == lbm.KERNEL_NODE         # 30*4 bytes is not a multiple of 16
     with lbm.Case(lbm.make_params(512, 4, 4, sides=lbm.SIDES_PERIODIC, storage="f32")) as c:
         assert c.step_kernel == lbm.KERNEL_NODE         # rows longer than 256
+    with lbm.Case(lbm.make_params(64, 8, 8, sides=lbm.SIDES_PERIODIC, storage="f16s")) as c:
+        with pytest.raises(lbm.LbmError):
+            c.set_step_kernel(lbm.KERNEL_ROW)           # 16-bit pairs: node kernel only
 
 
 # ---------------------------------------------------------------- reduced precision
