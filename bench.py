@@ -110,7 +110,13 @@ class ClockSampler:
                 if any(r[3].replace(".", "").isdigit() for r in rows) else None}
 
 
-def dist_setup():
+def dist_setup(backend: str = "nccl"):
+    """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK).  The
+    ranks are independent replicas; the process group carries only the
+    barriers around the timed region and the max over ranks of its time.
+    backend "gloo" runs the same plumbing on CPU (tests)."""
+    import datetime
+
     import torch
     import torch.distributed as dist
 
@@ -118,10 +124,12 @@ def dist_setup():
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
-        import datetime
-        torch.cuda.set_device(local)
-        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
-                                device_id=torch.device("cuda", local))
+        if backend == "nccl":
+            torch.cuda.set_device(local)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                    device_id=torch.device("cuda", local))
+        else:
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
     return rank, world, local
 
 
@@ -131,7 +139,8 @@ def max_over_ranks(x: float, world: int) -> float:
     import torch
     import torch.distributed as dist
 
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
@@ -355,7 +364,7 @@ def run_reference(args):
     return 0
 
 
-def main(argv=None):
+def parse_args(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=200)
@@ -370,6 +379,11 @@ def main(argv=None):
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3
+    return args
+
+
+def main(argv=None):
+    args = parse_args(argv)
     if args.impl == "reference":
         return run_reference(args)
     return run_engine(args)

@@ -8,7 +8,8 @@
 // (0.1 / (LY * 5.0))) and/or from --NAME value options; unset fields take
 // the reference's defaults.  Engine choices: --sides wall|periodic (default
 // wall, the reference's box), --storage f64|f32|f16s|bf16s (default f64),
-// --init rest|conduction, --seed, --amplitude, --device.
+// --collision bgk|regularized (default bgk, the reference's), --init
+// rest|conduction, --seed, --amplitude, --device.
 //
 // Behaviour of src/main.cu:11-93: CONTINUE_STEP = 0 starts from the rest
 // state of init_arrays (or the seeded conduction state with --init
@@ -298,8 +299,8 @@ struct Driver {
 void usage() {
     std::printf(
         "usage: rb3d [--params parameters.h] [--NAME value ...] [--sides wall|periodic]\n"
-        "            [--storage f64|f32|f16s|bf16s] [--init rest|conduction] [--seed N]\n"
-        "            [--amplitude A] [--device D] [--dry-run]\n"
+        "            [--storage f64|f32|f16s|bf16s] [--collision bgk|regularized]\n"
+        "            [--init rest|conduction] [--seed N] [--amplitude A] [--device D] [--dry-run]\n"
         "NAME is one of CONTINUE_STEP LX LY LZ NEND NDIAG NFLOWOUT NNUOUT RAYLEIGH PRANDTL\n"
         "T_HOT T_COLD GRAVITY BETA (src/parameters.h); values may be expressions.\n");
 }
@@ -310,7 +311,7 @@ int main(int argc, char **argv) {
     struct timeval start_time, end_time;
     gettimeofday(&start_time, nullptr);
     RunSurface rs;
-    std::string sides = "wall", storage = "f64", init = "rest";
+    std::string sides = "wall", storage = "f64", init = "rest", collision = "bgk";
     bool dry_run = false;
     unsigned long long seed = 1;
     double amplitude = 1e-3;
@@ -334,6 +335,7 @@ int main(int argc, char **argv) {
             if (key == "params") read_params_file(val, rs);
             else if (key == "sides") sides = val;
             else if (key == "storage") storage = val;
+            else if (key == "collision") collision = val;
             else if (key == "init") init = val;
             else if (key == "seed") seed = std::strtoull(val.c_str(), nullptr, 10);
             else if (key == "amplitude") amplitude = std::atof(val.c_str());
@@ -341,6 +343,8 @@ int main(int argc, char **argv) {
             else rs.set(key, val);
         }
         rs.resolve();
+        if (collision != "bgk" && collision != "regularized")
+            throw std::runtime_error("--collision must be bgk or regularized");
     } catch (const std::exception &e) {
         die(std::string("rb3d: ") + e.what());
     }
@@ -375,6 +379,8 @@ int main(int argc, char **argv) {
     }
 
     check(lbm_create(&d.p, &d.c), "lbm_create");
+    check(lbm_set_collision(d.c, collision == "regularized" ? LBM_COLLISION_REGULARIZED : LBM_COLLISION_BGK),
+          "lbm_set_collision");
     if (cont == 0) {
         if (init == "conduction") check(lbm_init_conduction(d.c, seed, amplitude, nullptr), "init");
         else check(lbm_init_rest(d.c, nullptr), "init");

@@ -121,3 +121,36 @@ def test_rb3d_writes_the_reference_files(lbm, oracle_mod, tmp_path, name):
     p = d / "statistics.dat"
     if want:
         np.testing.assert_allclose(_series(p.read_text()), _series(want), rtol=2e-6, atol=1e-20)
+
+
+def test_rb3d_rejects_unknown_collision(lbm):
+    r = subprocess.run([RB3D, "--dry-run", "--collision", "mrt"], capture_output=True, text=True)
+    assert r.returncode != 0 and "collision" in r.stderr
+
+
+@pytest.mark.gpu
+def test_rb3d_regularized_matches_library(lbm, tmp_path):
+    """rb3d --collision regularized writes the state the library computes
+    for the same case (FP64, closed box, seeded conduction start)."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from oracle import ref_run
+
+    c = dict(continue_step=0, lx=16, ly=12, lz=10, nend=40, rayleigh=1e6, prandtl=0.71)
+    (tmp_path / "parameters.h").write_text(params_h(c))
+    r = subprocess.run([RB3D, "--params", "parameters.h", "--collision", "regularized", "--init", "conduction",
+                        "--seed", "5", "--amplitude", "0.01"], cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    n = c["lx"] * c["ly"] * c["lz"]
+    st = ref_run.read_state(str(tmp_path / ref_run.case_dir(c)), c["nend"], n)
+    p = lbm.make_params(c["lx"], c["ly"], c["lz"], rayleigh=c["rayleigh"], prandtl=c["prandtl"],
+                        beta=0.01 / c["ly"], sides=lbm.SIDES_WALL, storage="f64")
+    with lbm.Case(p) as case:
+        case.set_collision("regularized")
+        case.init_conduction(5, 0.01)
+        case.step(c["nend"])
+        want = case.store_ref_state(("f", "g", "phi"))
+    for k in ("f", "g", "phi"):
+        assert np.array_equal(st[k], want[k].reshape(-1)), k
