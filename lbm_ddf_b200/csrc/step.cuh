@@ -480,12 +480,13 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
 }
 
 // Resident 128-thread blocks per SM the register allocation is sized for:
-// 2 (<= 255 registers) for FP64, which holds 54 doubles across the
-// collision; 4 (<= 128) for FP32 and 16-bit storage (B200, 256^3 FP16S with
+// 3 (<= 168 registers) for FP64, which holds 54 doubles across the
+// collision (B200, 256^3: 6.7, 7.4 and 6.6 GLUPS at 2, 3 and 4 blocks, the
+// last spilling); 4 (<= 128) for FP32 and 16-bit storage (256^3 FP16S with
 // interleaved pairs: 21.7 GLUPS at 4 blocks, 14.2 at 5 and 14.6 at 6, where
 // the update spills).
 template <class S> struct StepOccupancy {
-    static constexpr int value = sizeof(S) == 8 ? 2 : 4;
+    static constexpr int value = sizeof(S) == 8 ? 3 : 4;
 };
 
 // The whole update of one node: gather, moments, collision, carried
