@@ -150,6 +150,18 @@ def test_f64_matches_oracle(lbm, oracle_mod, periodic, steps):
     np.testing.assert_allclose(pa[:, 4] ** 2, pb[:, 4] ** 2, rtol=0, atol=1e-13)
 
 
+@pytest.mark.parametrize("periodic", [True, False])
+@pytest.mark.parametrize("lx,ly,lz", [(2, 3, 2), (3, 3, 2), (2, 4, 3), (33, 3, 2)])
+def test_f64_smallest_grids_bitwise(lbm, oracle_mod, periodic, lx, ly, lz):
+    """The smallest grids the C ABI accepts (LY = 3, two-node rows and
+    planes): every node touches a wall or wraps onto itself, in both
+    layouts; bitwise the oracle after 7 steps."""
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL, storage="f64")
+    got = engine_run(lbm, p, 7, seed=3, amplitude=1e-2)
+    o = oracle_run(oracle_mod, lx, ly, lz, 7, periodic, seed=3, amplitude=1e-2)
+    compare(got, o, 1e-12, bitwise=True)
+
+
 def test_f64_step_chunking_is_irrelevant(lbm):
     """7 steps in one call equals 3 + 1 + 3 calls (layout flag bookkeeping)."""
     p = lbm.make_params(16, 12, 10, sides=lbm.SIDES_WALL, storage="f64")
