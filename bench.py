@@ -12,9 +12,12 @@ engine arm (default): prints one JSON line with
   value      MLUPS over all ranks, populations resident in HBM, CUDA events on
              the launching stream around K steps, max over ranks;
   e2e        MLUPS of a whole job through the public API with host buffers:
-             restore the case from a page-locked host checkpoint, K steps each
-             followed by the observables (Nu, KE, ...) read back to the host,
-             save the case back to the host checkpoint;
+             restore the case from a page-locked host checkpoint, K steps
+             through lbm_step_observed one at a time, each returning to the
+             host the observables (Nu, KE, ...) of the state it started from
+             (reduced inside the step kernel), then the observables of the
+             final state, and save the case back to the host checkpoint: the
+             observables of every one of the K + 1 states reach the host;
   roofline   algorithmic bytes per launch (f and g read once and written
              once: 2*27*2 words per node) over the measured launch time,
              against the measured HBM copy bandwidth;
@@ -31,6 +34,7 @@ timing it prints, differenced between a 3-step and a longer run.
 from __future__ import annotations
 
 import argparse
+import ctypes
 import json
 import os
 import statistics
@@ -221,7 +225,8 @@ def run_engine(args):
     ms_per_step = secs / args.steps * 1e3
     value = world * nodes * args.steps / secs / 1e6
 
-    # e2e: host checkpoint -> K x (step + observables to host) -> host checkpoint
+    # e2e: host checkpoint -> K x (step, observables of its start state to
+    # host) -> observables of the final state -> host checkpoint
     nbytes = case.checkpoint_bytes()
     host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
     case.save_state(host, stream=stream)
@@ -231,8 +236,14 @@ def run_engine(args):
     barrier(world)
     t0 = time.perf_counter()
     e2e_case.restore_state(host, stream=stream)
+    fused = kind != lbm.KERNEL_ROW
     for _ in range(args.steps):
-        e2e_case.step(1, stream=stream)
+        if fused:
+            e2e_case.step_observed(1, stream=stream)
+        else:   # the row-staged kernel has no fused reduction
+            e2e_case.step(1, stream=stream)
+            e2e_case.observables(stream=stream)
+    if fused:
         e2e_case.observables(stream=stream)
     e2e_case.save_state(host, stream=stream)
     stream.synchronize()
@@ -240,7 +251,7 @@ def run_engine(args):
     barrier(world)
     e2e_secs = max_over_ranks(e2e_secs, world)
     e2e_value = world * nodes * args.steps / e2e_secs / 1e6
-    obs_bytes = 96
+    obs_bytes = ctypes.sizeof(lbm.LbmObservables) * (args.steps + (1 if fused else 0)) // args.steps
     e2e_case.close()
 
     # FP64 companion measurement (same workload, FP64 populations)
@@ -301,7 +312,10 @@ def run_engine(args):
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
                 "h2d_bytes_per_step": int(nbytes / args.steps),
                 "d2h_bytes_per_step": int(nbytes / args.steps) + obs_bytes,
-                "what": "restore from pinned host checkpoint, K x (step + observables to host), save to host"},
+                "what": ("restore from pinned host checkpoint, K x (step + observables of its start state "
+                         "to host, reduced in the step kernel), observables of the final state, save to host")
+                        if fused else
+                        "restore from pinned host checkpoint, K x (step + observables to host), save to host"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "algorithmic_bytes_per_lu": bytes_per_lu, "peak_source": peak_src},

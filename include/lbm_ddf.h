@@ -37,7 +37,7 @@
 extern "C" {
 #endif
 
-#define LBM_DDF_ABI_VERSION 2
+#define LBM_DDF_ABI_VERSION 3
 
 /* status codes */
 #define LBM_OK 0
@@ -214,6 +214,22 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
  * differ from the GPU's correctly rounded division by `divisor`.  A
  * diagnostic with no counterpart in the reference; expected result 0. */
 int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed, uint64_t *mismatches);
+
+/* Advances nsteps steps and returns, in out[0 .. nsteps) (host memory), the
+ * observables of every state the steps started from: out[i] is the state
+ * after (initial step count + i) steps, as lbm_get_observables would report
+ * it then.  For FP64 and FP32 storage each step kernel reduces them from
+ * the moments it computes anyway, so the per-step observables cost no extra
+ * read of the state (lbm_get_observables reads all populations once); for
+ * 16-bit storage, whose step is issue-bound, a separate reduction before
+ * each step measured faster and is used.  Call lbm_get_observables for the
+ * state after the last step.  Node kernel only
+ * (LBM_ERR_ARG if the case's step kernel is set to ROW); synchronises
+ * `stream`; LBM_ERR_DIVERGED if any entry saw a NaN/Inf (all entries are
+ * written).  The sums' order differs from lbm_get_observables', so results
+ * agree to rounding.  No counterpart in the reference (src/main.cu runs
+ * output_nu on stored fields every NNUOUT steps). */
+int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream);
 
 /* Chooses the step kernel of a case (LBM_KERNEL_*); LBM_ERR_ARG if the case
  * cannot use it.  lbm_get_step_kernel reports the one lbm_step launches. */

@@ -97,6 +97,7 @@ def lib() -> C.CDLL:
         L.lbm_store_ref_state.argtypes = [vp] + [_dp] * 7
         L.lbm_step.argtypes = [vp, C.c_int32, vp]
         L.lbm_get_observables.argtypes = [vp, C.POINTER(LbmObservables), vp]
+        L.lbm_step_observed.argtypes = [vp, C.c_int32, C.POINTER(LbmObservables), vp]
         L.lbm_get_profile.argtypes = [vp, _dp, vp]
         L.lbm_get_params.argtypes = [vp, P, C.POINTER(LbmDerived), C.POINTER(C.c_int64)]
         L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
@@ -123,7 +124,7 @@ def lib() -> C.CDLL:
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
                      "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
                      "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel",
-                     "lbm_set_collision", "lbm_get_collision",
+                     "lbm_set_collision", "lbm_get_collision", "lbm_step_observed",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
                      "lbm_batch_autotune"):
@@ -308,6 +309,15 @@ class Case:
         if rc != OK and not (allow_diverged and rc == ERR_DIVERGED):
             check(rc)
         return o.as_dict()
+
+    def step_observed(self, n: int = 1, stream=None, allow_diverged: bool = False) -> list:
+        """n steps; returns the observables of each state the steps started
+        from (reduced inside the step kernels: no extra read of the state)."""
+        out = (LbmObservables * max(1, n))()
+        rc = lib().lbm_step_observed(self._h, int(n), out, _stream_handle(stream))
+        if rc != OK and not (allow_diverged and rc == ERR_DIVERGED):
+            check(rc)
+        return [out[i].as_dict() for i in range(n)]
 
     @property
     def step_kernel(self) -> int:

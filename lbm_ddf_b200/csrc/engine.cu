@@ -54,7 +54,7 @@ size_t store_bytes(int storage) {
 using namespace lbm_internal;
 
 namespace {
-constexpr int kObs = 13;           // partial sums per block, see obs_kernel
+constexpr int kObs = lbm::kObsTerms;   // partial sums per block (step.cuh add_obs_terms)
 constexpr int kObsThreads = 256;
 constexpr int kStepThreads = 128;
 }  // namespace
@@ -63,12 +63,6 @@ constexpr int kStepThreads = 128;
 // device kernels besides the step
 // ---------------------------------------------------------------------------
 namespace lbm {
-
-__device__ __forceinline__ double warp_sum(double v) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
 
 // Per-block partial sums, in FP64, of
 //   0 uy*phi  1 |u|^2  2 ux  3 uy  4 uz  5 phi
@@ -92,21 +86,7 @@ __global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, d
         else
             gather<S, SWAPPED, false>(a, g, fr, gr);
         const Moments<R> m = node_moments<S>(a, fr, gr, n);
-        const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
-        acc[0] += uy * phi;
-        acc[1] += ux * ux + uy * uy + uz * uz;
-        acc[2] += ux;
-        acc[3] += uy;
-        acc[4] += uz;
-        acc[5] += phi;
-        if (g.iy == 0) acc[6] += phi;
-        if (g.iy == 1) acc[7] += phi;
-        if (g.iy == 2) acc[8] += phi;
-        if (g.iy == a.ly - 1) acc[9] += phi;
-        if (g.iy == a.ly - 2) acc[10] += phi;
-        if (g.iy == a.ly - 3) acc[11] += phi;
-        if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)m.rho))
-            acc[12] += 1.0;
+        add_obs_terms(acc, m, g.iy, a.ly);
     }
     __shared__ double red[kObs][kObsThreads / 32];
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -162,6 +142,22 @@ __global__ void __launch_bounds__(32 * kObs) obs_finalize(const double *__restri
         out->diverged = tot[12] > 0.0 ? 1 : 0;
         out->reserved = 0;
     }
+}
+
+// The per-block rows a fused step kernel wrote, summed in blocks of
+// kRowChunk rows into one partial row each (warp w sums term w, lane l the
+// rows l, l + 32, ... of the chunk, then a butterfly over the lanes): a
+// fixed order, so the result is deterministic.  Launch: kObs warps.
+constexpr int kRowChunk = 1024;
+__global__ void __launch_bounds__(32 * kObs) obs_rows_reduce(const double *__restrict__ rows, int nrows,
+                                                             double *__restrict__ partial) {
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int r0 = blockIdx.x * kRowChunk;
+    const int r1 = min(nrows, r0 + kRowChunk);
+    double s = 0.0;
+    for (int r = r0 + lane; r < r1; r += 32) s += rows[(size_t)r * kObs + w];
+    s = warp_sum(s);
+    if (lane == 0) partial[(size_t)blockIdx.x * kObs + w] = s;
 }
 
 // Vertical profile, src/output.cu:336-368: one block per xz plane iy.
@@ -380,6 +376,7 @@ template <class S> StepArgs<S> make_args(const lbm_case *c) {
     for (int b = 0; b < 3; b++)
         a.pairs[b] = a.pairs_st[b] = (S *)c->f + (size_t)(9 * b) * (size_t)c->ps * elem_stride<S>();
     a.pair_row = (uint32_t)c->ps;
+    a.obs_rows = nullptr;
     a.phip = (typename Codec<S>::P *)c->phip;
     a.lx = c->p.lx;
     a.ly = c->p.ly;
@@ -417,12 +414,27 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
     return fail(LBM_ERR_ARG, "bad storage");
 }
 
-template <class S, bool SW, bool PER> void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+template <class S, bool SW, bool PER, bool OBS = false>
+void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
     const unsigned grid = grid_for(c->nodes, kStepThreads);
     if (c->collision == LBM_COLLISION_REGULARIZED)
-        step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED><<<grid, kStepThreads, 0, st>>>(a);
+        step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED, OBS><<<grid, kStepThreads, 0, st>>>(a);
     else
-        step_kernel<S, SW, PER, LBM_COLLISION_BGK><<<grid, kStepThreads, 0, st>>>(a);
+        step_kernel<S, SW, PER, LBM_COLLISION_BGK, OBS><<<grid, kStepThreads, 0, st>>>(a);
+}
+
+// One node-kernel step that also writes the observables of the state it
+// reads as per-block rows into a.obs_rows.
+template <class S> void launch_step_observed(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    static_assert(sizeof(S) > 2, "16-bit steps reduce their observables in a separate pass");
+    const bool per = c->p.sides == LBM_SIDES_PERIODIC;
+    if (c->swapped) {
+        if (per) launch_step_t<S, true, true, true>(c, a, st);
+        else launch_step_t<S, true, false, true>(c, a, st);
+    } else {
+        if (per) launch_step_t<S, false, true, true>(c, a, st);
+        else launch_step_t<S, false, false, true>(c, a, st);
+    }
 }
 
 // Whether the row-staged kernel (rowstep.cuh) can run this case: periodic
@@ -586,6 +598,8 @@ int lbm_destroy(lbm_case *c) {
     cudaFree(c->partial);
     cudaFree(c->d_obs);
     cudaFree(c->d_err);
+    cudaFree(c->obs_rows);
+    cudaFree(c->obs_series);
     delete c;
     return LBM_OK;
 }
@@ -780,6 +794,74 @@ int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
     CUDA_TRY(cudaStreamSynchronize(st));
     if (err) return fail(LBM_ERR_CUDA, "a step kernel gave up waiting for its shared-memory copies");
     if (out->diverged) return fail(LBM_ERR_DIVERGED, "NaN/Inf in the macroscopic fields");
+    return LBM_OK;
+}
+
+int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream) {
+    int rc = check_mutable(c, true);
+    if (rc) return rc;
+    if (nsteps < 0) return fail(LBM_ERR_ARG, "nsteps < 0");
+    if (nsteps > 0 && !out) return fail(LBM_ERR_ARG, "out is NULL");
+    if (use_row_kernel(c))
+        return fail(LBM_ERR_ARG, "steps with observables run on the node kernel; the case's step kernel is set to ROW");
+    if (nsteps == 0) return LBM_OK;
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int rows = (int)grid_for(c->nodes, kStepThreads);
+    const int parts = (rows + kRowChunk - 1) / kRowChunk;
+    if (!c->obs_rows) {   // per-block rows, then the chunk partials behind them
+        CUDA_TRY(cudaMalloc(&c->obs_rows, (size_t)(rows + parts) * kObs * sizeof(double)));
+    }
+    if (nsteps > c->obs_series_cap) {
+        if (c->obs_series) {
+            CUDA_TRY(cudaStreamSynchronize(st));
+            cudaFree(c->obs_series);
+            c->obs_series = nullptr;
+            c->obs_series_cap = 0;
+        }
+        CUDA_TRY(cudaMalloc(&c->obs_series, (size_t)nsteps * sizeof(lbm_observables)));
+        c->obs_series_cap = nsteps;
+    }
+    double *partial = c->obs_rows + (size_t)rows * kObs;
+    rc = with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        StepArgs<S> a = make_args<S>(c);
+        a.obs_rows = c->obs_rows;
+        ObsConsts k;
+        k.nodes = (double)c->nodes;
+        k.plane = (double)c->p.lx * (double)c->p.lz;
+        k.ly = (double)c->p.ly;
+        k.diff = c->d.diff;
+        k.dT = c->p.t_hot - c->p.t_cold;
+        k.visc = c->d.visc;
+        for (int s = 0; s < nsteps; s++) {
+            k.step = c->step + s;   // the state this step starts from
+            if constexpr (sizeof(S) == 2) {
+                // 16-bit storage: the step is issue-bound, and folding the
+                // reduction into it cost more (B200, 256^3: +0.43 ms per
+                // step) than a separate pass over the state (0.30-0.40 ms)
+                LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
+                obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, c->obs_series + s);
+                launch_step<S>(c, a, st);
+            } else {
+                launch_step_observed<S>(c, a, st);
+                obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial);
+                obs_finalize<<<1, 32 * kObs, 0, st>>>(partial, parts, k, c->obs_series + s);
+            }
+            c->swapped = !c->swapped;
+            c->rest_phi = false;
+            a.use_phi_fix = 0;
+        }
+        return LBM_OK;
+    });
+    if (rc) return rc;
+    c->step += nsteps;
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, c->obs_series, (size_t)nsteps * sizeof(lbm_observables), cudaMemcpyDeviceToHost,
+                             st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (int s = 0; s < nsteps; s++)
+        if (out[s].diverged) return fail(LBM_ERR_DIVERGED, "NaN/Inf in the macroscopic fields");
     return LBM_OK;
 }
 

@@ -105,6 +105,7 @@ template <class S> struct StepArgs {
         return reinterpret_cast<typename Pack16<SS>::T *>(pairs_st[k / 9])[(uint32_t)(k % 9) * pair_row +
                                                                            (uint32_t)j];
     }
+    double *obs_rows;  // fused observables: one row of kObsTerms sums per block (else unused)
     S *pairs[3];       // 16-bit storage: rows 0, 9 and 18 of the (f, g) pair array
     S *pairs_st[3];    // the same, for the stores (see fs)
     uint32_t pair_row; // pairs per row (the padded node count)
@@ -491,6 +492,85 @@ template <class S> struct StepOccupancy {
 
 // The whole update of one node: gather, moments, collision, carried
 // temperature, scatter.
+// ---- observables of a node's moments --------------------------------------
+//
+// FP64 sums of
+//   0 uy*phi  1 |u|^2  2 ux  3 uy  4 uz  5 phi
+//   6..8  phi on the planes iy = 0, 1, 2
+//   9..11 phi on the planes iy = LY-1, LY-2, LY-3
+//   12 number of nodes with a non-finite moment
+// (src/output.cu:199-256 and :24-34 reduce the same fields on the host).
+constexpr int kObsTerms = 13;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+template <class R>
+__device__ __forceinline__ void add_obs_terms(double (&acc)[kObsTerms], const Moments<R> &m, int iy, int ly) {
+    const double ux = m.ux, uy = m.uy, uz = m.uz, phi = m.phi;
+    acc[0] += uy * phi;
+    acc[1] += ux * ux + uy * uy + uz * uz;
+    acc[2] += ux;
+    acc[3] += uy;
+    acc[4] += uz;
+    acc[5] += phi;
+    if (iy == 0) acc[6] += phi;
+    if (iy == 1) acc[7] += phi;
+    if (iy == 2) acc[8] += phi;
+    if (iy == ly - 1) acc[9] += phi;
+    if (iy == ly - 2) acc[10] += phi;
+    if (iy == ly - 3) acc[11] += phi;
+    if (!isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)m.rho))
+        acc[12] += 1.0;
+}
+
+// The block's sums of the kObsTerms terms of its nodes into row[0 ..
+// kObsTerms); every thread of the block calls it, `valid` false for threads
+// past the last node.  Each thread brings its node's six dense terms (0-5)
+// and plane; per warp, the six are summed by butterflies; the plane terms
+// are the warp's phi sum when all its nodes lie in one plane (rows of a
+// multiple of 32 nodes), else butterflies too; the non-finite count is a
+// ballot.  Then the warps' sums are added in warp order.
+template <int BLOCK>
+__device__ __forceinline__ void block_obs_row(const double (&d)[6], int iy, bool valid, bool bad, int ly,
+                                              double *__restrict__ row) {
+    __shared__ double red[kObsTerms][BLOCK / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    double w[kObsTerms];
+#pragma unroll
+    for (int k = 0; k < 6; k++) w[k] = warp_sum(d[k]);
+    const int iy0 = __shfl_sync(0xffffffffu, iy, 0);   // lane 0 holds a node if any lane does
+    const int planes[6] = {0, 1, 2, ly - 1, ly - 2, ly - 3};
+    if (__all_sync(0xffffffffu, !valid || iy == iy0)) {
+#pragma unroll
+        for (int k = 0; k < 6; k++) w[6 + k] = iy0 == planes[k] ? w[5] : 0.0;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 6; k++) w[6 + k] = warp_sum(valid && iy == planes[k] ? d[5] : 0.0);
+    }
+    w[12] = (double)__popc(__ballot_sync(0xffffffffu, valid && bad));
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < kObsTerms; k++) red[k][warp] = w[k];
+    }
+    __syncthreads();
+    if (threadIdx.x < kObsTerms) {
+        double t = 0.0;
+        for (int v = 0; v < BLOCK / 32; v++) t += red[threadIdx.x][v];
+        row[threadIdx.x] = t;
+    }
+}
+
+// The moments a node update starts from (the observables of the state the
+// step reads) and the node's plane.
+template <class R> struct NodeOut {
+    Moments<R> m;
+    int32_t iy;
+};
+
 // ---- 16-bit storage: the collision in the stored, normalised variables ----
 //
 // FP16S / BF16S rows hold (fh_i, gh_i) pairs, fh_i = f_i / w_i and
@@ -602,7 +682,7 @@ __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const fl
 }
 
 template <class S, bool SWAPPED, bool PERIODIC, class A>
-__device__ __forceinline__ void update_node_norm(const A &a, uint32_t n) {
+__device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t n) {
     const Node g = make_node<PERIODIC>(a, n);
     float fh[Q], gh[Q];
     const bool interior = PERIODIC && g.vym && g.vyp;
@@ -618,13 +698,13 @@ __device__ __forceinline__ void update_node_norm(const A &a, uint32_t n) {
         scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho);
     else
         scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho);
+    return {m, g.iy};
 }
 
 template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A>
-__device__ __forceinline__ void update_node(const A &a, uint32_t n) {
+__device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a, uint32_t n) {
     if constexpr (sizeof(S) == 2 && COLL == LBM_COLLISION_BGK) {
-        update_node_norm<S, SWAPPED, PERIODIC>(a, n);
-        return;
+        return update_node_norm<S, SWAPPED, PERIODIC>(a, n);
     }
     using R = typename Codec<S>::R;
     const Node g = make_node<PERIODIC>(a, n);
@@ -643,13 +723,39 @@ __device__ __forceinline__ void update_node(const A &a, uint32_t n) {
         scatter<S, SWAPPED, PERIODIC, true>(a, g, fr, gr, m.rho);
     else
         scatter<S, SWAPPED, PERIODIC, false>(a, g, fr, gr, m.rho);
+    return {m, g.iy};
 }
 
-template <class S, bool SWAPPED, bool PERIODIC, int COLL>
+// One time step.  With OBS, the kernel also reduces the observables of the
+// state it reads — the moments every node update computes anyway — into one
+// row of kObsTerms FP64 sums per block (a.obs_rows), at no extra read of the
+// populations.
+template <class S, bool SWAPPED, bool PERIODIC, int COLL, bool OBS = false>
 __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
-    if (n >= a.nodes) return;
-    update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
+    if constexpr (!OBS) {
+        if (n >= a.nodes) return;
+        update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
+    } else {
+        // the terms of add_obs_terms: uy*phi, |u|^2, ux, uy, uz, phi
+        double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        int iy = 0;
+        bool bad = false;
+        const bool valid = n < a.nodes;
+        if (valid) {
+            const auto o = update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
+            const double ux = o.m.ux, uy = o.m.uy, uz = o.m.uz, phi = o.m.phi;
+            d[0] = uy * phi;
+            d[1] = ux * ux + uy * uy + uz * uz;
+            d[2] = ux;
+            d[3] = uy;
+            d[4] = uz;
+            d[5] = phi;
+            iy = o.iy;
+            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)o.m.rho);
+        }
+        block_obs_row<128>(d, iy, valid, bad, a.ly, a.obs_rows + (size_t)blockIdx.x * kObsTerms);
+    }
 }
 
 }  // namespace lbm

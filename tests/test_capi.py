@@ -31,7 +31,7 @@ def test_exports_every_declared_symbol(lbm):
 
 
 def test_abi_version(lbm):
-    assert lbm.lib().lbm_abi_version() == 2
+    assert lbm.lib().lbm_abi_version() == 3
 
 
 def test_largest_16bit_case_accepted(lbm):
