@@ -28,8 +28,8 @@ def test_oracle_subcritical_conduction(oracle_mod):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("storage,tol", [("f64", 3e-3), ("f32", 3e-3), ("f16s", 5e-3), ("bf16s", 0.1)])
-def test_subcritical_conduction(lbm, storage, tol):
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "bf16s"])
+def test_subcritical_conduction(lbm, storage):
     import torch
 
     if not torch.cuda.is_available():
@@ -41,11 +41,19 @@ def test_subcritical_conduction(lbm, storage, tol):
         a = c.observables()
         c.step(1000)
         b = c.observables()
-    if storage == "bf16s":   # 8-bit mantissas: plate temperatures off by ~2^-9, Nu by a few %
-        for k in ("nu_bulk", "nu_top", "nu_bottom"):
-            assert abs(b[k] - 1.0) <= tol, (k, b[k])
+    if storage in ("f16s", "bf16s"):
+        # Near the plates the stored g/w - t0 is close to +-1/2, where FP16
+        # spaces values 2^-11 apart and BF16 2^-8, against plane-to-plane
+        # temperature differences of 1/16 here: the plate gradients, and so
+        # the plate Nu, are off by up to ~4% (FP16S) and ~20% (BF16S); the
+        # bulk flux is not.  At convecting Ra the plate gradients are tens of
+        # times larger and the error a few percent or less.
+        plate = {"f16s": 0.05, "bf16s": 0.25}[storage]
+        assert abs(b["nu_bulk"] - 1.0) <= 0.01, b["nu_bulk"]
+        for k in ("nu_top", "nu_bottom"):
+            assert abs(b[k] - 1.0) <= plate, (k, b[k])
     else:
-        _steady_conduction(a, b, tol)
+        _steady_conduction(a, b, 3e-3)
 
 
 @pytest.mark.gpu
