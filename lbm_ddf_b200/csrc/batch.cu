@@ -51,6 +51,7 @@ template <class S> struct BatchCase {
     FastDiv div_lx, div_ly;
     R tau, tauc, rcp_tau, rcp_tauc, rcp_rt;
     R omega_f, omega_g, force_fac, gb, t0, t_hot, t_cold, phi_fix;
+    R t_top, t_dy;       // 16-bit storage: the conduction-profile shift (step.cuh shift0)
     int32_t use_phi_fix, pad;
 
     // element (k * ps + j) * elem_stride of the population array, indexed
@@ -176,6 +177,8 @@ template <class S> BatchCase<S> describe(const lbm_case *c) {
     d.force_fac = (R)(1.0 - 0.5 / c->d.tau);
     d.gb = (R)(c->p.gravity * c->p.beta);
     d.t0 = (R)c->d.t0;
+    d.t_top = (R)(c->p.t_hot - (c->p.t_hot - c->p.t_cold) * 0.5 / c->p.ly);
+    d.t_dy = (R)((c->p.t_hot - c->p.t_cold) / c->p.ly);
     d.t_hot = (R)c->p.t_hot;
     d.t_cold = (R)c->p.t_cold;
     d.phi_fix = (R)0.5;

@@ -215,8 +215,13 @@ __global__ void export_pop_kernel(const StepArgs<S> a, int which, int k, double 
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if (K == k) {
+            // 16-bit storage: g/w is stored relative to the conduction
+            // profile at the location read (step.cuh shift0)
+            float sh = 0.f;
+            if constexpr (elem_stride<S>() == 2) sh = shift0(a, g) + read_shift_delta<SWAPPED, K, false>(a, g);
             if (which)
-                v = (double)C::template g_in<K>(load_pop<S, SWAPPED, K, false, 1>(a, g), a.t0);
+                v = (double)C::template g_in<K>(load_pop<S, SWAPPED, K, false, 1>(a, g),
+                                                elem_stride<S>() == 2 ? (typename C::R)sh : a.t0);
             else
                 v = (double)C::template f_in<K>(load_pop<S, SWAPPED, K, false, 0>(a, g), a.t0);
         }
@@ -249,12 +254,16 @@ __global__ void import_pop_kernel(const StepArgs<S> a, int which, int k, const d
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.nodes) return;
     const double v = in[n];
+    // 16-bit storage: shifted by the conduction profile at this node (natural layout)
+    const uint32_t q = a.div_lx.div(n);
+    const int iy = (int)(q - a.div_ly.div(q) * (uint32_t)a.ly);
+    const float sh = fmaf(-(float)iy, (float)a.t_dy, (float)a.t_top);
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if (K == k) {
             using R = typename C::R;
             if (which)
-                a.st(1, K, n) = C::template g_out<K>((R)v, a.t0);
+                a.st(1, K, n) = C::template g_out<K>((R)v, elem_stride<S>() == 2 ? (R)sh : a.t0);
             else
                 a.st(0, K, n) = C::template f_out<K>((R)v, a.t0);
         }
@@ -287,10 +296,12 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
     if (n >= a.nodes) return;
     double t = 0.5;
+    const uint32_t q = a.div_lx.div(n);
+    const uint32_t z = a.div_ly.div(q);
+    const int iy = (int)(q - z * (uint32_t)a.ly);
+    // 16-bit storage: g/w stored relative to the conduction profile here (step.cuh shift0)
+    const float sh = fmaf(-(float)iy, (float)a.t_dy, (float)a.t_top);
     if (mode == 1) {
-        const uint32_t q = a.div_lx.div(n);
-        const uint32_t z = a.div_ly.div(q);
-        const int iy = (int)(q - z * (uint32_t)a.ly);
         const uint64_t r = splitmix64(seed_key + (uint64_t)n);
         const double u = (double)(r >> 11) * (1.0 / 9007199254740992.0);
         t = __dsub_rn(t_hot, __ddiv_rn(__dmul_rn(__dsub_rn(t_hot, t_cold), (double)iy), __dsub_rn((double)a.ly, 1.0)));
@@ -300,7 +311,7 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
         constexpr int K = decltype(kk)::value;
         const double gk = __dmul_rn(wd(K), t);
         a.st(0, K, n) = C::template f_out<K>((R)0, a.t0);
-        a.st(1, K, n) = C::template g_out<K>((R)gk, a.t0);
+        a.st(1, K, n) = C::template g_out<K>((R)gk, elem_stride<S>() == 2 ? (R)sh : a.t0);
     });
     a.phip[n] = (typename C::P)t;
 }
@@ -394,6 +405,8 @@ template <class S> StepArgs<S> make_args(const lbm_case *c) {
     a.force_fac = (R)(1.0 - 0.5 / c->d.tau);
     a.gb = (R)(c->p.gravity * c->p.beta);
     a.t0 = (R)c->d.t0;
+    a.t_top = (R)(c->p.t_hot - (c->p.t_hot - c->p.t_cold) * 0.5 / c->p.ly);
+    a.t_dy = (R)((c->p.t_hot - c->p.t_cold) / c->p.ly);
     a.t_hot = (R)c->p.t_hot;
     a.t_cold = (R)c->p.t_cold;
     a.use_phi_fix = c->rest_phi ? 1 : 0;
@@ -891,7 +904,7 @@ int lbm_get_profile(lbm_case *c, double *out, void *stream) {
 
 // Checkpoint image: header, f, g, phip (each region 256-byte aligned).
 struct CheckpointHeader {
-    char magic[8];          // "LBMDDF2\0" (16-bit states hold interleaved (f, g) pairs)
+    char magic[8];          // "LBMDDF3\0" (16-bit states: interleaved (f, g) pairs, g shifted by the conduction profile)
     lbm_params p;
     int64_t step;
     int32_t swapped;
@@ -926,7 +939,7 @@ int lbm_save_state(lbm_case *c, void *host, uint64_t bytes, void *stream) {
     DeviceGuard dg(c->p.device);
     CheckpointHeader h;
     std::memset(&h, 0, sizeof h);
-    std::memcpy(h.magic, "LBMDDF2", 8);
+    std::memcpy(h.magic, "LBMDDF3", 8);
     h.p = c->p;
     h.step = c->step;
     h.swapped = c->swapped ? 1 : 0;
@@ -953,7 +966,7 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
     if (!host || bytes < need) return fail(LBM_ERR_ARG, "checkpoint buffer missing or too small");
     CheckpointHeader h;
     std::memcpy(&h, host, sizeof h);
-    if (std::memcmp(h.magic, "LBMDDF2", 8) != 0) return fail(LBM_ERR_ARG, "not an engine checkpoint");
+    if (std::memcmp(h.magic, "LBMDDF3", 8) != 0) return fail(LBM_ERR_ARG, "not an engine checkpoint");
     if (h.p.lx != c->p.lx || h.p.ly != c->p.ly || h.p.lz != c->p.lz || h.p.storage != c->p.storage ||
         h.p.sides != c->p.sides || h.ps != c->ps || h.p.rayleigh != c->p.rayleigh || h.p.prandtl != c->p.prandtl ||
         h.p.beta != c->p.beta || h.p.gravity != c->p.gravity || h.p.t_hot != c->p.t_hot || h.p.t_cold != c->p.t_cold)

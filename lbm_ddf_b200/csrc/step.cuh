@@ -69,6 +69,9 @@ template <class S> struct StepArgs {
     R force_fac;       // 1 - 1/(2 tau)
     R gb;              // gravity*beta
     R t0, t_hot, t_cold;
+    // 16-bit storage shifts g/w by the conduction profile at the node a value
+    // is stored at, T_c(iy) = t_top - iy * t_dy (see stored_shift)
+    R t_top, t_dy;
     // The reference's rest state (src/initial.cu:218-240) stores phi = 0.5
     // while its populations w_i * 0.5 sum to 0.5 - 2^-54; its first step
     // collides with the stored 0.5.  When set, the moments use phi_fix
@@ -191,16 +194,47 @@ __device__ __forceinline__ typename Pack16<S>::T load_pair(const A &a, const Nod
     return a.ld2(K, g.n);
 }
 
+// 16-bit storage keeps g_i / w_i - T_c at every location, T_c(iy) =
+// T_hot - (T_hot - T_cold) (iy + 1/2) / LY the conduction profile at the
+// plane of the node the value is stored at (halfway walls: the plates sit
+// half a node outside the first and last planes).  Near the plates, where Nu
+// is measured, g/w is then close to the stored shift and 16-bit rounding
+// small against the plane-to-plane temperature step; with one constant
+// shift it was up to 2^-11 (FP16) and 2^-8 (BF16) there.  Inside a node
+// update the g values are kept relative to the node's own T_c (shift0); a
+// value read from or written to a neighbour's plane differs from that by
+// a multiple of t_dy:
+//   read (swapped layout, population K from x - c_K): + c_Ky t_dy
+//   write (swapped layout, population I to x + c_I):   + c_Iy t_dy
+// and by nothing at the node itself (natural layout, bounce-back).
+template <class A> __device__ __forceinline__ float shift0(const A &a, const Node &g) {
+    return fmaf(-(float)g.iy, (float)a.t_dy, (float)a.t_top);
+}
+template <bool SWAPPED, int K, bool INTERIOR, class A>
+__device__ __forceinline__ float read_shift_delta(const A &a, const Node &g) {
+    constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
+    if constexpr (!SWAPPED || DY == 0) return 0.f;
+    else return inside_t<INTERIOR, DX, DY, DZ>(g) ? (float)cy(K) * (float)a.t_dy : 0.f;
+}
+template <bool SWAPPED, int I, bool INTERIOR, class A>
+__device__ __forceinline__ float write_shift_delta(const A &a, const Node &g) {
+    constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
+    if constexpr (!SWAPPED || DY == 0) return 0.f;
+    else return inside_t<INTERIOR, DX, DY, DZ>(g) ? (float)cy(I) * (float)a.t_dy : 0.f;
+}
+
 template <class S, bool SWAPPED, bool INTERIOR = false, class A>
 __device__ __forceinline__ void gather(const A &a, const Node &g, typename Codec<S>::R (&fr)[Q],
                                        typename Codec<S>::R (&gr)[Q]) {
     using C = Codec<S>;
+    float s0 = 0.f;
+    if constexpr (elem_stride<S>() == 2) s0 = shift0(a, g);
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: Codec's f_in / g_in on the unpacked values
+        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: f_i = w_i fh, g_i = w_i (gh + T_c at the location)
             const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
             fr[K] = (float)wd(K) * v.x;
-            gr[K] = (float)wd(K) * (v.y + a.t0);
+            gr[K] = (float)wd(K) * (v.y + (s0 + read_shift_delta<SWAPPED, K, INTERIOR>(a, g)));
         } else {
             fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g), a.t0);
             gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g), a.t0);
@@ -455,6 +489,8 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
                                         const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
     using C = Codec<S>;
     using R = typename C::R;
+    float s0 = 0.f;
+    if constexpr (elem_stride<S>() == 2) s0 = shift0(a, g);
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
@@ -463,8 +499,10 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
-        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: Codec's f_out / g_out, packed
-            const auto v = Pack16<S>::pack(fv * (float)winv(I), fmaf(gv, (float)winv(I), -a.t0));
+        if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: f/w and g/w - T_c at the location, packed
+            // the location's T_c is s0 - write_shift_delta (it is s0 at the node itself)
+            const float sl = s0 - write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
+            const auto v = Pack16<S>::pack(fv * (float)winv(I), fmaf(gv, (float)winv(I), -sl));
             if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
                 a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
             else
@@ -574,7 +612,8 @@ template <class R> struct NodeOut {
 // ---- 16-bit storage: the collision in the stored, normalised variables ----
 //
 // FP16S / BF16S rows hold (fh_i, gh_i) pairs, fh_i = f_i / w_i and
-// gh_i = g_i / w_i - t0, one 32-bit word per population and node.  The
+// gh_i = g_i / w_i - T_c (T_c the conduction profile at the location, see
+// shift0), one 32-bit word per population and node.  The
 // update below works on those directly (FP32 arithmetic): the moments sum
 // them per weight class and weight the four class sums, and the BGK steps in
 // normalised form,
@@ -590,12 +629,14 @@ __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&f
         constexpr int K = decltype(kk)::value;
         const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
         fh[K] = v.x;
-        gh[K] = v.y;
+        gh[K] = v.y + read_shift_delta<SWAPPED, K, INTERIOR>(a, g);   // relative to the node's T_c
     });
 }
 
+// gh here is g/w - s0 (s0 the node's conduction-profile temperature); t0 is
+// the mean temperature of the force term.
 __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], const float (&gh)[Q], float phip,
-                                                       float gbeta, float t0) {
+                                                       float gbeta, float t0, float s0) {
     float r[4] = {0.f, 0.f, 0.f, 0.f}, x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f},
           z[4] = {0.f, 0.f, 0.f, 0.f}, t[4] = {0.f, 0.f, 0.f, 0.f};
     Unroll<0, Q>::run([&](auto kk) {
@@ -616,7 +657,7 @@ __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], con
     m.ux = fmaf(w3, x[3], fmaf(w2, x[2], w1 * x[1]));
     const float jy = fmaf(w3, y[3], fmaf(w2, y[2], w1 * y[1]));
     m.uz = fmaf(w3, z[3], fmaf(w2, z[2], w1 * z[1]));
-    m.phi = fmaf(w3, t[3], fmaf(w2, t[2], fmaf(w1, t[1], w0 * t[0]))) + t0;   // sum w_i (gh_i + t0)
+    m.phi = fmaf(w3, t[3], fmaf(w2, t[2], fmaf(w1, t[1], w0 * t[0]))) + s0;   // sum w_i (gh_i + s0)
     m.uy = jy + 0.5f * (gbeta * (phip - t0));
     return m;
 }
@@ -624,11 +665,12 @@ __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], con
 // Both relaxations as affine maps of the old value, with per-node
 // coefficients (k = kf (c_y - u_y) takes three values, one per c_y):
 //   fh* = (1 - om_f) fh + (om_f rho + k) + (om_f + k) p
-//   gh* = (1 - om_g) gh + om_g (phi - t0) + om_g phi p
+//   gh* = (1 - om_g) gh + om_g (phi - s0) + om_g phi p
 // and p_I, p_J = (q +/- 2 eu) / 2 with q = eu^2 - 3 u^2 for a pair of
 // opposite directions: two multiply-adds per population and three per pair.
+// (gh = g/w - s0; t0 enters only the buoyancy force.)
 __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
-                                             float om_g, float force_fac, float gbeta, float t0) {
+                                             float om_g, float force_fac, float gbeta, float t0, float s0) {
     const float ux3 = 3.f * m.ux, uy3 = 3.f * m.uy, uz3 = 3.f * m.uz;
     const float uv = 3.f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
     const float kf = 3.f * force_fac * (gbeta * (m.phi - t0));
@@ -636,7 +678,7 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
     const float af = 1.f - om_f, orho = om_f * m.rho;
     const float c0[3] = {orho + k_m, orho + k_0, orho + k_p};    // indexed by c_y + 1
     const float c1[3] = {om_f + k_m, om_f + k_0, om_f + k_p};
-    const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - t0);
+    const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - s0);
     auto relax = [&](float &f, float &g, float p, int cy1) {
         f = fmaf(af, f, fmaf(c1[cy1], p, c0[cy1]));
         g = fmaf(ag, g, fmaf(d1, p, d0));
@@ -665,14 +707,15 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
 // 32-bit store of the packed (f, g) pair per population.
 template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
 __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float (&fh)[Q], const float (&gh)[Q],
-                                             float rho) {
+                                             float rho, float s0) {
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
         float gv = gh[I];
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
-        if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * a.t0;
+        if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
+        gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);   // relative to T_c at the location written
         const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
             a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -690,14 +733,15 @@ __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t 
         gather_norm<S, SWAPPED, true>(a, g, fh, gh);
     else
         gather_norm<S, SWAPPED, false>(a, g, fh, gh);
-    Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0);
+    const float s0 = shift0(a, g);
+    Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0, s0);
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0);
+    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0);
     a.phip[n] = m.phi;
     if (interior)
-        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho);
+        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
     else
-        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho);
+        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho, s0);
     return {m, g.iy};
 }
 

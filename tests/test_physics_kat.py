@@ -12,10 +12,10 @@ import numpy as np
 import pytest
 
 
-def _steady_conduction(obs_a, obs_b, tol):
+def _steady_conduction(obs_a, obs_b, tol, drift=1e-6):
     for k in ("nu_bulk", "nu_top", "nu_bottom"):
         assert abs(obs_b[k] - 1.0) <= tol, (k, obs_b[k])
-        assert abs(obs_b[k] - obs_a[k]) <= 1e-6, k    # no longer changing
+        assert abs(obs_b[k] - obs_a[k]) <= drift, k    # no longer changing (to storage rounding)
 
 
 def test_oracle_subcritical_conduction(oracle_mod):
@@ -41,19 +41,11 @@ def test_subcritical_conduction(lbm, storage):
         a = c.observables()
         c.step(1000)
         b = c.observables()
-    if storage in ("f16s", "bf16s"):
-        # Near the plates the stored g/w - t0 is close to +-1/2, where FP16
-        # spaces values 2^-11 apart and BF16 2^-8, against plane-to-plane
-        # temperature differences of 1/16 here: the plate gradients, and so
-        # the plate Nu, are off by up to ~4% (FP16S) and ~20% (BF16S); the
-        # bulk flux is not.  At convecting Ra the plate gradients are tens of
-        # times larger and the error a few percent or less.
-        plate = {"f16s": 0.05, "bf16s": 0.25}[storage]
-        assert abs(b["nu_bulk"] - 1.0) <= 0.01, b["nu_bulk"]
-        for k in ("nu_top", "nu_bottom"):
-            assert abs(b[k] - 1.0) <= plate, (k, b[k])
-    else:
-        _steady_conduction(a, b, 3e-3)
+    # 16-bit storage keeps g/w relative to the conduction profile, so the
+    # plate gradients of this state are resolved (with one constant shift
+    # the plate Nu were off by ~4% in FP16S and ~20% in BF16S here)
+    tol, drift = {"f64": (3e-3, 1e-6), "f32": (3e-3, 1e-6), "f16s": (4e-3, 1e-5), "bf16s": (1e-2, 1e-3)}[storage]
+    _steady_conduction(a, b, tol, drift)
 
 
 @pytest.mark.gpu
