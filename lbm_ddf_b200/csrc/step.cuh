@@ -629,7 +629,12 @@ __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&f
         constexpr int K = decltype(kk)::value;
         const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
         fh[K] = v.x;
-        gh[K] = v.y + read_shift_delta<SWAPPED, K, INTERIOR>(a, g);   // relative to the node's T_c
+        gh[K] = v.y;
+        // relative to the node's T_c; on interior rows of the swapped layout
+        // the read and write re-referencing is folded into the collision
+        // (collide_norm's `fold`), as the moments do not see it (the deltas
+        // of each weight class sum to zero)
+        if constexpr (!(INTERIOR && SWAPPED)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
     });
 }
 
@@ -668,9 +673,14 @@ __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], con
 //   gh* = (1 - om_g) gh + om_g (phi - s0) + om_g phi p
 // and p_I, p_J = (q +/- 2 eu) / 2 with q = eu^2 - 3 u^2 for a pair of
 // opposite directions: two multiply-adds per population and three per pair.
-// (gh = g/w - s0; t0 enters only the buoyancy force.)
+// (gh = g/w - s0; t0 enters only the buoyancy force.)  fold: the plane
+// spacing of the conduction profile when gh holds raw stored values that
+// were read from, and go to, the planes y - c_y and y + c_y (interior rows,
+// swapped layout): ag (v + c_y fold) + ... + c_y fold = ag v + ... +
+// (ag + 1) c_y fold, one more coefficient per c_y; else 0.
 __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
-                                             float om_g, float force_fac, float gbeta, float t0, float s0) {
+                                             float om_g, float force_fac, float gbeta, float t0, float s0,
+                                             float fold) {
     const float ux3 = 3.f * m.ux, uy3 = 3.f * m.uy, uz3 = 3.f * m.uz;
     const float uv = 3.f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
     const float kf = 3.f * force_fac * (gbeta * (m.phi - t0));
@@ -679,9 +689,11 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
     const float c0[3] = {orho + k_m, orho + k_0, orho + k_p};    // indexed by c_y + 1
     const float c1[3] = {om_f + k_m, om_f + k_0, om_f + k_p};
     const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - s0);
+    const float df = (ag + 1.f) * fold;
+    const float d0c[3] = {d0 - df, d0, d0 + df};                    // indexed by c_y + 1
     auto relax = [&](float &f, float &g, float p, int cy1) {
         f = fmaf(af, f, fmaf(c1[cy1], p, c0[cy1]));
-        g = fmaf(ag, g, fmaf(d1, p, d0));
+        g = fmaf(ag, g, fmaf(d1, p, d0c[cy1]));
     };
     relax(fh[0], gh[0], -0.5f * uv, 1);
     Unroll<1, Q>::run([&](auto ii) {
@@ -715,7 +727,9 @@ __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const fl
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
-        gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);   // relative to T_c at the location written
+        // relative to T_c at the location written (folded into the
+        // collision on interior rows of the swapped layout)
+        if constexpr (!(INTERIOR && SWAPPED)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
         const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
             a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -736,7 +750,8 @@ __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t 
     const float s0 = shift0(a, g);
     Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0, s0);
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0);
+    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
+                 SWAPPED && interior ? (float)a.t_dy : 0.f);
     a.phip[n] = m.phi;
     if (interior)
         scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
