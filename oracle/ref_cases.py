@@ -17,6 +17,9 @@ REF_CASES = {
                       rayleigh=1.0e5, prandtl=0.71),
     "w24_s1000": dict(lx=24, ly=16, lz=20, continue_step=100, nend=1100, ndiag=100, nnuout=100,
                       rayleigh=1.0e5, prandtl=0.71),
+    # long run at the 64^3 benchmark grid (Ra 1e5): 10,000 steps from a seeded state
+    "c0_s10000": dict(lx=64, ly=64, lz=64, continue_step=100, nend=10100, nnuout=1000,
+                      rayleigh=1.0e5, prandtl=0.71),
     # timing cases: 256^3, Ra 1e7 (and 64^3, Ra 1e5) from the rest state
     "c1_n3": dict(lx=256, ly=256, lz=256, continue_step=0, nend=3, rayleigh=1.0e7, prandtl=0.71),
     "c1_n53": dict(lx=256, ly=256, lz=256, continue_step=0, nend=53, rayleigh=1.0e7, prandtl=0.71),
