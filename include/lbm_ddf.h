@@ -265,9 +265,10 @@ int lbm_batch_add(lbm_batch *b, lbm_case *c);
 int lbm_batch_remove(lbm_batch *b, lbm_case *c);
 int lbm_batch_size(const lbm_batch *b, int32_t *members, uint64_t *nodes);
 int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream);
-/* Launch shape: tile (= block) of 128 or 256 nodes; blocks_per_sm > 0 runs
- * that many persistent blocks per SM walking the tile list, 0 one block per
- * tile; use_graph replays captured graphs for multi-step calls. */
+/* Launch shape: blocks of 128 or 256 threads, each tile 4 x block nodes of
+ * one member; blocks_per_sm > 0 runs that many persistent blocks per SM
+ * walking the tile list, 0 one block per tile; use_graph replays captured
+ * graphs for multi-step calls. */
 int lbm_batch_set_config(lbm_batch *b, int32_t block, int32_t blocks_per_sm, int32_t use_graph);
 int lbm_batch_get_config(const lbm_batch *b, int32_t *block, int32_t *blocks_per_sm, int32_t *use_graph);
 /* Times every launch shape on 2 x steps_per_trial real steps of the batch

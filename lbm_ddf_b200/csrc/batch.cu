@@ -5,7 +5,7 @@
 // AA layout and collision model; one launch of batch_step_kernel per
 // non-empty group (normally one: members move through the layouts in step)
 // advances the group's members by one step.  Their nodes are cut into tiles
-// of BLOCK nodes, numbered case after case; blocks walk the tile list with a
+// of kTileRounds x BLOCK nodes, numbered case after case; blocks walk the tile list with a
 // grid stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block
 // per tile), find each tile's case by a binary search over the tiles' prefix
 // sums held in shared memory, and apply the same node update as the
@@ -37,6 +37,11 @@ using namespace lbm_internal;
 namespace lbm {
 
 constexpr int kMaxBatch = 2048;    // members per batch (tile prefix sums in shared memory)
+// A tile is kTileRounds rounds of BLOCK nodes of one member, so the member
+// lookup (binary search, descriptor) is paid once per kTileRounds nodes a
+// thread updates (96-case FP16S ensemble on B200: 19.3, 19.9, 20.5 and 20.6
+// GLUPS at 1, 2, 4 and 8 rounds; FP32 unchanged).
+constexpr int kTileRounds = 4;
 
 // Per-member descriptor, read by every block that works on the member.
 // It provides what update_node needs (the accessor interface of StepArgs).
@@ -103,8 +108,12 @@ __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
             else hi = mid;
         }
         const BatchCase<S> &cs = cases[lo];
-        const uint32_t u = (t - s_start[lo]) * BLOCK + threadIdx.x;
-        if (u < cs.nodes) update_node<S, SWAPPED, true, COLL>(cs, u);
+        const uint32_t u0 = (t - s_start[lo]) * (BLOCK * kTileRounds) + threadIdx.x;
+#pragma unroll 1
+        for (int r = 0; r < kTileRounds; r++) {
+            const uint32_t u = u0 + r * BLOCK;
+            if (u < cs.nodes) update_node<S, SWAPPED, true, COLL>(cs, u);
+        }
     }
 }
 
@@ -240,7 +249,8 @@ int refresh(lbm_batch *b, cudaStream_t st) {
             const BatchCase<S> d = describe<S>(order[(size_t)i]);
             std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
             b->h_start[i] = tiles;
-            tiles += (uint32_t)((order[(size_t)i]->nodes + b->block - 1) / b->block);
+            const int64_t tile = (int64_t)b->block * kTileRounds;
+            tiles += (uint32_t)((order[(size_t)i]->nodes + tile - 1) / tile);
         }
         return LBM_OK;
     });
