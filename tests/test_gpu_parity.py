@@ -4,7 +4,7 @@ and with the CPU oracle.
 Tolerances (field-relative, max|a-b| / max|b|):
   FP64 storage      bitwise equal populations and macroscopic fields (the
                     FP64 path rounds exactly as the reference binary does);
-                    the north-star bounds 1e-12 (fields) and 1e-10 (Nu) are
+                    the parity bounds 1e-12 (fields) and 1e-10 (Nu) are
                     asserted as well; Nu from the device reduction 1e-10
   FP32 storage      5e-5 after <= 200 steps (FP32 arithmetic)
   FP16S / BF16S     5e-3 / 4e-2 after <= 100 steps (16-bit storage)

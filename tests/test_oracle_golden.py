@@ -6,7 +6,7 @@ through its restart path from seeded states (tests/golden/make_golden.py).
 This pins the oracle: with its default contraction model (the multiply-adds
 nvcc fuses in the reference build, lbm_oracle.c) every population and every
 macroscopic field is bitwise equal to the reference's after 1, 2, 50 and 1000
-steps; the north-star bounds (1e-12 field-relative, Nu 1e-10) are checked as
+steps; the parity bounds (1e-12 field-relative, Nu 1e-10) are checked as
 well, and the reference's printed Nu lines (7 significant digits) are
 reproduced.
 """
