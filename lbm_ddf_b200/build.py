@@ -20,7 +20,8 @@ LIB = os.path.join(PKG, "liblbm_ddf.so")
 DRIVER = os.path.join(PKG, "rb3d")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr"]
+NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",
+              "-Werror", "all-warnings"]  # a warning (e.g. the address of a temporary) fails the build
 LIB_SOURCES = ["engine.cu", "batch.cu"]
 HEADERS = ["lattice.cuh", "step.cuh", "bulk.cuh", "rowstep.cuh", "internal.h"]
 
