@@ -12,6 +12,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -467,16 +468,19 @@ bool use_row_kernel(const lbm_case *c) { return c->kernel == LBM_KERNEL_ROW; }
 
 template <class S, bool SW, int PITCH>
 cudaError_t launch_row_p(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
-    static bool configured = false;   // per instantiation; the attribute is per device function
+    // The shared-memory attribute belongs to the function in one device's
+    // context: one bit per device (per instantiation), set once it is applied.
+    static std::atomic<uint64_t> configured{0};
     const size_t smem = row_smem_bytes<S>(PITCH);
-    if (!configured) {
+    const uint64_t bit = c->p.device < 64 ? uint64_t(1) << c->p.device : 0;
+    if (!(configured.load(std::memory_order_acquire) & bit)) {
         cudaError_t e = cudaFuncSetAttribute(row_step_kernel<S, SW, PITCH>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        configured = true;
+        configured.fetch_or(bit, std::memory_order_release);
     }
     row_step_kernel<S, SW, PITCH><<<(unsigned)(c->p.ly * c->p.lz), (unsigned)c->p.lx, smem, st>>>(a, c->d_err);
-    return cudaSuccess;
+    return cudaPeekAtLastError();
 }
 
 template <class S, bool SW> cudaError_t launch_row_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
@@ -485,13 +489,10 @@ template <class S, bool SW> cudaError_t launch_row_t(const lbm_case *c, const St
     return launch_row_p<S, SW, 256>(c, a, st);
 }
 
-template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+// One step of the case's kernel; returns the launch's error, if any.
+template <class S> cudaError_t launch_step(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
     if constexpr (elem_stride<S>() == 1) {
-        if (use_row_kernel(c)) {
-            if (c->swapped) launch_row_t<S, true>(c, a, st);
-            else launch_row_t<S, false>(c, a, st);
-            return;
-        }
+        if (use_row_kernel(c)) return c->swapped ? launch_row_t<S, true>(c, a, st) : launch_row_t<S, false>(c, a, st);
     }
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
@@ -501,6 +502,7 @@ template <class S> void launch_step(const lbm_case *c, const StepArgs<S> &a, cud
         if (per) launch_step_t<S, false, true>(c, a, st);
         else launch_step_t<S, false, false>(c, a, st);
     }
+    return cudaPeekAtLastError();
 }
 
 // Dispatch a (SWAPPED, PERIODIC)-templated launch for the case's current layout.
@@ -765,15 +767,20 @@ int lbm_step(lbm_case *c, int32_t nsteps, void *stream) {
         using S = std::remove_pointer_t<decltype(tag)>;
         StepArgs<S> a = make_args<S>(c);
         for (int s = 0; s < nsteps; s++) {
-            launch_step<S>(c, a, st);
+            const cudaError_t e = launch_step<S>(c, a, st);
+            if (e != cudaSuccess) {
+                c->step += s;   // the steps launched before the failure
+                cudaGetLastError();
+                return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+            }
             c->swapped = !c->swapped;
             c->rest_phi = false;
             a.use_phi_fix = 0;
         }
+        c->step += nsteps;
         return LBM_OK;
     });
     if (rc) return rc;
-    c->step += nsteps;
     CUDA_TRY(cudaGetLastError());
     return LBM_OK;
 }
@@ -855,7 +862,7 @@ int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *s
                 // step) than a separate pass over the state (0.30-0.40 ms)
                 LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
                 obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, c->obs_series + s);
-                launch_step<S>(c, a, st);
+                (void)launch_step<S>(c, a, st);   // a launch error is read after the loop
             } else {
                 launch_step_observed<S>(c, a, st);
                 obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial);
