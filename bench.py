@@ -11,13 +11,17 @@ flush is needed between steps.
 engine arm (default): prints one JSON line with
   value      MLUPS over all ranks, populations resident in HBM, CUDA events on
              the launching stream around K steps, max over ranks;
-  e2e        MLUPS of a whole job through the public API with host buffers:
-             restore the case from a page-locked host checkpoint, K steps
-             through lbm_step_observed one at a time, each returning to the
-             host the observables (Nu, KE, ...) of the state it started from
-             (reduced inside the step kernel), then the observables of the
-             final state, and save the case back to the host checkpoint: the
-             observables of every one of the K + 1 states reach the host;
+  e2e        MLUPS of a whole new run through the public API with host
+             buffers: the seeded temperature field copied in from page-locked
+             host memory (lbm_init_temperature: equilibrium populations from
+             it), K steps through lbm_step_observed one at a time, each
+             returning to the host the observables (Nu, KE, ...) of the state
+             it started from (reduced inside the step kernel), then the
+             observables of the final state: the observables of every one of
+             the K + 1 states reach the host;
+  e2e_resume the same K steps as a resumed run: the whole state restored
+             from a page-locked host checkpoint first and saved back to it
+             at the end (host<->device copies of the full state);
   roofline   algorithmic bytes per launch (f and g read once and written
              once: 2*27*2 words per node) over the measured launch time,
              against the measured HBM copy bandwidth;
@@ -194,6 +198,7 @@ def time_steps(case, stream, steps: int):
 
 
 def run_engine(args):
+    import numpy as np
     import torch
 
     import lbm_ddf_b200 as lbm
@@ -225,34 +230,59 @@ def run_engine(args):
     ms_per_step = secs / args.steps * 1e3
     value = world * nodes * args.steps / secs / 1e6
 
-    # e2e: host checkpoint -> K x (step, observables of its start state to
-    # host) -> observables of the final state -> host checkpoint
-    nbytes = case.checkpoint_bytes()
-    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    case.save_state(host, stream=stream)
-    torch.cuda.synchronize()
+    # Two whole jobs through the public API with host buffers, each: input
+    # from pinned host memory -> K x (step, observables of its start state to
+    # the host) -> observables of the final state.
+    #   e2e         a new run: the seeded conduction temperature field (made
+    #               on the host, outside the timed region) copied in by
+    #               init_temperature, populations at equilibrium from it;
+    #   e2e_resume  a resumed run: the whole state restored from a host
+    #               checkpoint, and saved back to it at the end.
+    fused = kind != lbm.KERNEL_ROW
+
+    def job_steps(c):
+        for _ in range(args.steps):
+            if fused:
+                c.step_observed(1, stream=stream)
+            else:   # the row-staged kernel has no fused reduction
+                c.step(1, stream=stream)
+                c.observables(stream=stream)
+        if fused:
+            c.observables(stream=stream)
+
+    obs_bytes = ctypes.sizeof(lbm.LbmObservables) * (args.steps + (1 if fused else 0)) // args.steps
+    tdtype = np.float64 if p.storage == lbm.STORE_F64 else np.float32
+    temp = torch.from_numpy(lbm.conduction_temperature(w["lx"], w["ly"], w["lz"], 1000 + rank, 1e-3,
+                                                       dtype=tdtype)).pin_memory()
     e2e_case = lbm.Case(p)
     e2e_case.set_step_kernel(kind)
     barrier(world)
     t0 = time.perf_counter()
-    e2e_case.restore_state(host, stream=stream)
-    fused = kind != lbm.KERNEL_ROW
-    for _ in range(args.steps):
-        if fused:
-            e2e_case.step_observed(1, stream=stream)
-        else:   # the row-staged kernel has no fused reduction
-            e2e_case.step(1, stream=stream)
-            e2e_case.observables(stream=stream)
-    if fused:
-        e2e_case.observables(stream=stream)
-    e2e_case.save_state(host, stream=stream)
+    e2e_case.init_temperature(temp, stream=stream)
+    job_steps(e2e_case)
     stream.synchronize()
-    e2e_secs = time.perf_counter() - t0
-    barrier(world)
-    e2e_secs = max_over_ranks(e2e_secs, world)
+    e2e_secs = max_over_ranks(time.perf_counter() - t0, world)
     e2e_value = world * nodes * args.steps / e2e_secs / 1e6
-    obs_bytes = ctypes.sizeof(lbm.LbmObservables) * (args.steps + (1 if fused else 0)) // args.steps
+    temp_bytes = temp.numel() * temp.element_size()
     e2e_case.close()
+    del temp
+
+    nbytes = case.checkpoint_bytes()
+    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+    case.save_state(host, stream=stream)
+    torch.cuda.synchronize()
+    res_case = lbm.Case(p)
+    res_case.set_step_kernel(kind)
+    barrier(world)
+    t0 = time.perf_counter()
+    res_case.restore_state(host, stream=stream)
+    job_steps(res_case)
+    res_case.save_state(host, stream=stream)
+    stream.synchronize()
+    res_secs = max_over_ranks(time.perf_counter() - t0, world)
+    res_value = world * nodes * args.steps / res_secs / 1e6
+    res_case.close()
+    del host
 
     # FP64 companion measurement (same workload, FP64 populations)
     f64 = None
@@ -310,12 +340,17 @@ def run_engine(args):
                    "step_kernel": kernel_used,
                    "parallelism": f"replicas x{world}"},
         "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
-                "h2d_bytes_per_step": int(nbytes / args.steps),
-                "d2h_bytes_per_step": int(nbytes / args.steps) + obs_bytes,
-                "what": ("restore from pinned host checkpoint, K x (step + observables of its start state "
-                         "to host, reduced in the step kernel), observables of the final state, save to host")
-                        if fused else
-                        "restore from pinned host checkpoint, K x (step + observables to host), save to host"},
+                "h2d_bytes_per_step": int(temp_bytes / args.steps),
+                "d2h_bytes_per_step": obs_bytes,
+                "what": "new run: seeded temperature field from pinned host memory (init_temperature: "
+                        "equilibrium populations), K x (step + observables of its start state to host"
+                        + (", reduced in the step kernel" if fused and lbm.STORAGE_BYTES[p.storage] > 2 else "")
+                        + "), observables of the final state"},
+        "e2e_resume": {"value": round(res_value, 2), "unit": "MLUPS",
+                       "h2d_bytes_per_step": int(nbytes / args.steps),
+                       "d2h_bytes_per_step": int(nbytes / args.steps) + obs_bytes,
+                       "what": "resumed run: whole state restored from a pinned host checkpoint, K x (step + "
+                               "observables to host), observables of the final state, state saved to host"},
         "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                      "frac": round(achieved / peak, 4), "traffic": traffic,
                      "algorithmic_bytes_per_lu": bytes_per_lu, "peak_source": peak_src},

@@ -7,7 +7,7 @@
  *   - the compile-time fields of src/parameters.h:5-31      -> lbm_params
  *   - the derived globals of src/globals.cu:13-23            -> lbm_derive
  *   - initialize() / init_arrays, src/initial.cu:3-241       -> lbm_create,
- *     lbm_init_rest, lbm_init_conduction
+ *     lbm_init_rest, lbm_init_conduction, lbm_init_temperature
  *   - the restart reader, src/initial.cu:110-205             -> lbm_load_ref_state
  *   - the six launches and two copies of one step,
  *     src/main.cu:27-46                                      -> lbm_step
@@ -135,6 +135,16 @@ int lbm_init_rest(lbm_case *c, void *stream);
  * splitmix64(splitmix64(seed) + idx); zero velocity; f = 0 and g_i = w_i T
  * (equilibria); carried previous temperature = T. */
 int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stream);
+
+/* The same state from the caller's temperature field: zero velocity, f = 0,
+ * g_i = w_i T and carried previous temperature = T, with T[idx] (idx =
+ * (iz*LY + iy)*LX + ix, the reference's node order) copied from `temperature`
+ * — host (pinned or pageable) or device memory, in the carried-temperature
+ * type: double for F64 storage, float otherwise.  With the T that
+ * lbm_init_conduction forms it gives that call's state bit for bit in F64
+ * storage.  The reference starts from its rest state (init_arrays) or a
+ * restart file only. */
+int lbm_init_temperature(lbm_case *c, const void *temperature, void *stream);
 
 /* Restart state from host FP64 arrays in the reference's file layout
  * (%09d.dat = rho,ux,uy,uz,phi and fg%09d.dat = f,g; src/initial.cu:110-205).

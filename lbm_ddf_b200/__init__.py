@@ -93,6 +93,7 @@ def lib() -> C.CDLL:
         L.lbm_destroy.argtypes = [vp]
         L.lbm_init_rest.argtypes = [vp, vp]
         L.lbm_init_conduction.argtypes = [vp, C.c_uint64, C.c_double, vp]
+        L.lbm_init_temperature.argtypes = [vp, vp, vp]
         L.lbm_load_ref_state.argtypes = [vp] + [_dp] * 7
         L.lbm_store_ref_state.argtypes = [vp] + [_dp] * 7
         L.lbm_step.argtypes = [vp, C.c_int32, vp]
@@ -206,6 +207,33 @@ def make_params(lx, ly, lz, rayleigh=1e5, prandtl=0.71, t_hot=1.0, t_cold=0.0, g
                      gravity=gravity, beta=beta)
 
 
+def _splitmix64(x: np.ndarray) -> np.ndarray:
+    """splitmix64 finaliser (Steele, Lea & Flood 2014) on a uint64 array."""
+    x = x + np.uint64(0x9E3779B97F4A7C15)
+    x = (x ^ (x >> np.uint64(30))) * np.uint64(0xBF58476D1CE4E5B9)
+    x = (x ^ (x >> np.uint64(27))) * np.uint64(0x94D049BB133111EB)
+    return x ^ (x >> np.uint64(31))
+
+
+def conduction_temperature(lx: int, ly: int, lz: int, seed: int, amplitude: float = 1e-3,
+                           t_hot: float = 1.0, t_cold: float = 0.0, dtype=np.float64) -> np.ndarray:
+    """The temperature field lbm_init_conduction forms, on the host: the
+    conduction profile T_hot - ((T_hot - T_cold) iy) / (LY - 1) plus
+    amplitude (2u - 1), u = splitmix64(splitmix64(seed) + idx) / 2^64 (53
+    bits), in the same FP64 operations, as a flat array in the reference's
+    node order (x fastest).  Pass it (as float32 for non-FP64 storage) to
+    Case.init_temperature, perturbed as a study needs."""
+    n = lx * ly * lz
+    key = _splitmix64(np.array([seed], dtype=np.uint64))[0]
+    with np.errstate(over="ignore"):
+        r = _splitmix64(np.arange(n, dtype=np.uint64) + key)
+    u = (r >> np.uint64(11)).astype(np.float64) * (1.0 / 9007199254740992.0)
+    iy = np.broadcast_to(np.arange(ly, dtype=np.float64)[None, :, None], (lz, ly, lx)).reshape(-1)
+    t = t_hot - ((t_hot - t_cold) * iy) / (ly - 1.0)
+    t = t + amplitude * (2.0 * u - 1.0)
+    return t.astype(dtype, copy=False)
+
+
 def derive(p: LbmParams) -> dict:
     d = LbmDerived()
     check(lib().lbm_derive(C.byref(p), C.byref(d)))
@@ -283,6 +311,29 @@ class Case:
 
     def init_conduction(self, seed: int, amplitude: float = 1e-3, stream=None):
         check(lib().lbm_init_conduction(self._h, C.c_uint64(seed), amplitude, _stream_handle(stream)))
+
+    def init_temperature(self, temperature, stream=None):
+        """Start from a temperature field (C ABI lbm_init_temperature): zero
+        velocity, equilibrium populations.  `temperature` holds LZ*LY*LX
+        values in the reference's node order (x fastest), float64 for F64
+        storage and float32 otherwise: a numpy array or a torch tensor on the
+        host (pinned for an asynchronous copy) or on this case's GPU."""
+        want = np.float64 if self.params.storage == STORE_F64 else np.float32
+        n = self.n
+        if hasattr(temperature, "data_ptr"):
+            if str(temperature.dtype) != "torch." + np.dtype(want).name or not temperature.is_contiguous():
+                raise ValueError(f"temperature must be a contiguous {np.dtype(want).name} tensor")
+            if temperature.numel() != n:
+                raise ValueError(f"temperature has {temperature.numel()} values, the grid {n}")
+            ptr = int(temperature.data_ptr())
+            keep = temperature
+        else:
+            keep = np.ascontiguousarray(temperature, dtype=want).reshape(-1)
+            if keep.size != n:
+                raise ValueError(f"temperature has {keep.size} values, the grid {n}")
+            ptr = int(keep.ctypes.data)
+        check(lib().lbm_init_temperature(self._h, C.c_void_p(ptr), _stream_handle(stream)))
+        del keep   # the call returns once the state is written
 
     def load_ref_state(self, rho, ux, uy, uz, phi, f, g):
         arrs = [np.ascontiguousarray(a, dtype=np.float64).reshape(-1) for a in (rho, ux, uy, uz, phi, f, g)]

@@ -285,7 +285,8 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
     return x ^ (x >> 31);
 }
 
-// Conduction (mode 1) or rest (mode 0, src/initial.cu:208-241) state.
+// Conduction (mode 1), rest (mode 0, src/initial.cu:208-241) or given
+// temperature (mode 2: T = a.phip[n], copied there by the caller) state.
 // Temperatures are formed in FP64 with explicit round-to-nearest operations,
 // in the order T = T_hot - ((T_hot - T_cold) * iy) / (LY - 1.0), then
 // T + amplitude*(2u - 1), so every build gives the same bits.
@@ -307,6 +308,8 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
         const double u = (double)(r >> 11) * (1.0 / 9007199254740992.0);
         t = __dsub_rn(t_hot, __ddiv_rn(__dmul_rn(__dsub_rn(t_hot, t_cold), (double)iy), __dsub_rn((double)a.ly, 1.0)));
         t = __dadd_rn(t, __dmul_rn(amplitude, __dsub_rn(__dmul_rn(2.0, u), 1.0)));
+    } else if (mode == 2) {
+        t = (double)a.phip[n];
     }
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
@@ -651,6 +654,16 @@ int lbm_init_rest(lbm_case *c, void *stream) { return init_common(c, 0, 0, 0.0, 
 
 int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stream) {
     return init_common(c, 1, seed, amplitude, stream);
+}
+
+int lbm_init_temperature(lbm_case *c, const void *temperature, void *stream) {
+    int rc = check_mutable(c, false);
+    if (rc) return rc;
+    if (!temperature) return fail(LBM_ERR_ARG, "temperature is NULL");
+    DeviceGuard dg(c->p.device);
+    const size_t bytes = (size_t)c->nodes * (c->p.storage == LBM_STORE_F64 ? sizeof(double) : sizeof(float));
+    CUDA_TRY(cudaMemcpyAsync(c->phip, temperature, bytes, cudaMemcpyDefault, (cudaStream_t)stream));
+    return init_common(c, 2, 0, 0.0, stream);
 }
 
 int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const double *uy, const double *uz,
