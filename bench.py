@@ -14,9 +14,10 @@ engine arm (default): prints one JSON line with
   e2e        MLUPS of a whole new run through the public API with host
              buffers: the seeded temperature field copied in from page-locked
              host memory (lbm_init_temperature: equilibrium populations from
-             it), K steps through lbm_step_observed one at a time, each
-             returning to the host the observables (Nu, KE, ...) of the state
-             it started from (reduced inside the step kernel), then the
+             it), K steps through lbm_step_observed_async one at a time, each
+             copying to page-locked host memory the observables (Nu, KE, ...)
+             of the state it started from (reduced inside the step kernel),
+             which the host reads while the next step runs, then the
              observables of the final state: the observables of every one of
              the K + 1 states reach the host;
   e2e_resume the same K steps as a resumed run: the whole state restored
@@ -239,16 +240,26 @@ def run_engine(args):
     #   e2e_resume  a resumed run: the whole state restored from a host
     #               checkpoint, and saved back to it at the end.
     fused = kind != lbm.KERNEL_ROW
+    obs_buf = lbm.ObservablesBuffer(args.steps)
+    events = [torch.cuda.Event(), torch.cuda.Event()]
 
-    def job_steps(c):
-        for _ in range(args.steps):
-            if fused:
-                c.step_observed(1, stream=stream)
-            else:   # the row-staged kernel has no fused reduction
-                c.step(1, stream=stream)
-                c.observables(stream=stream)
-        if fused:
-            c.observables(stream=stream)
+    def job_steps(c, steps=args.steps):
+        # Each step's observables are copied to page-locked host memory and
+        # read by the host one step later, while the next step runs, so the
+        # GPU does not wait for the host between steps.
+        for s in range(steps + 1):
+            if s < steps:
+                if fused:
+                    c.step_observed_async(1, obs_buf, first=s, stream=stream)
+                    events[s % 2].record(stream)
+                else:   # the row-staged kernel has no fused reduction
+                    c.observables(stream=stream)
+                    c.step(1, stream=stream)
+            if fused and s > 0:
+                events[(s - 1) % 2].synchronize()
+                if obs_buf[s - 1]["diverged"]:
+                    raise RuntimeError(f"diverged at step {s - 1}")
+        c.observables(stream=stream)
 
     obs_bytes = ctypes.sizeof(lbm.LbmObservables) * (args.steps + (1 if fused else 0)) // args.steps
     tdtype = np.float64 if p.storage == lbm.STORE_F64 else np.float32
@@ -256,6 +267,11 @@ def run_engine(args):
                                                        dtype=tdtype)).pin_memory()
     e2e_case = lbm.Case(p)
     e2e_case.set_step_kernel(kind)
+    # untimed warm-up job: first launches of the observed-step kernels and
+    # the case's reduction buffers, as for the device-timed steps
+    e2e_case.init_temperature(temp, stream=stream)
+    job_steps(e2e_case, min(args.warmup, args.steps))
+    stream.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     e2e_case.init_temperature(temp, stream=stream)
@@ -273,6 +289,9 @@ def run_engine(args):
     torch.cuda.synchronize()
     res_case = lbm.Case(p)
     res_case.set_step_kernel(kind)
+    res_case.restore_state(host, stream=stream)
+    job_steps(res_case, min(args.warmup, args.steps))
+    stream.synchronize()
     barrier(world)
     t0 = time.perf_counter()
     res_case.restore_state(host, stream=stream)
@@ -343,7 +362,8 @@ def run_engine(args):
                 "h2d_bytes_per_step": int(temp_bytes / args.steps),
                 "d2h_bytes_per_step": obs_bytes,
                 "what": "new run: seeded temperature field from pinned host memory (init_temperature: "
-                        "equilibrium populations), K x (step + observables of its start state to host"
+                        "equilibrium populations), K x (step + observables of its start state to pinned host "
+                        "memory, read by the host one step later"
                         + (", reduced in the step kernel" if fused and lbm.STORAGE_BYTES[p.storage] > 2 else "")
                         + "), observables of the final state"},
         "e2e_resume": {"value": round(res_value, 2), "unit": "MLUPS",

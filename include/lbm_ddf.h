@@ -241,6 +241,17 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
  * output_nu on stored fields every NNUOUT steps). */
 int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream);
 
+/* lbm_step_observed without waiting: enqueues the steps and the copy of
+ * their observables into out[0 .. nsteps) on `stream` and returns, so a
+ * host loop keeps the GPU busy while it reads earlier entries.  `out` is
+ * page-locked host memory (an asynchronous copy; pageable memory works but
+ * the copy then blocks) or device memory; it is valid once the stream has
+ * passed the call (synchronise it, or record an event after the call and
+ * wait on that).  The caller checks out[i].diverged.  Successive calls on
+ * one case reuse one device buffer in stream order, so they run on one
+ * stream (or the caller orders the streams). */
+int lbm_step_observed_async(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream);
+
 /* Chooses the step kernel of a case (LBM_KERNEL_*); LBM_ERR_ARG if the case
  * cannot use it.  lbm_get_step_kernel reports the one lbm_step launches. */
 int lbm_set_step_kernel(lbm_case *c, int32_t kind);

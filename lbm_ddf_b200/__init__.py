@@ -99,6 +99,7 @@ def lib() -> C.CDLL:
         L.lbm_step.argtypes = [vp, C.c_int32, vp]
         L.lbm_get_observables.argtypes = [vp, C.POINTER(LbmObservables), vp]
         L.lbm_step_observed.argtypes = [vp, C.c_int32, C.POINTER(LbmObservables), vp]
+        L.lbm_step_observed_async.argtypes = [vp, C.c_int32, vp, vp]
         L.lbm_get_profile.argtypes = [vp, _dp, vp]
         L.lbm_get_params.argtypes = [vp, P, C.POINTER(LbmDerived), C.POINTER(C.c_int64)]
         L.lbm_checkpoint_bytes.argtypes = [vp, C.POINTER(C.c_uint64)]
@@ -125,7 +126,7 @@ def lib() -> C.CDLL:
                      "lbm_get_observables", "lbm_get_profile", "lbm_get_params", "lbm_checkpoint_bytes",
                      "lbm_save_state", "lbm_restore_state", "lbm_selfcheck_division",
                      "lbm_observables_noalloc", "lbm_set_step_kernel", "lbm_get_step_kernel",
-                     "lbm_set_collision", "lbm_get_collision", "lbm_step_observed",
+                     "lbm_set_collision", "lbm_get_collision", "lbm_step_observed", "lbm_step_observed_async",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
                      "lbm_batch_autotune"):
@@ -266,6 +267,29 @@ def case_bytes(p: LbmParams) -> int:
     return int(b.value)
 
 
+class ObservablesBuffer:
+    """n lbm_observables records in page-locked host memory (torch's pinned
+    allocator), the destination of Case.step_observed_async."""
+
+    def __init__(self, n: int):
+        import torch
+
+        self._mem = torch.empty(max(1, n) * C.sizeof(LbmObservables), dtype=torch.uint8, pin_memory=True)
+        self._recs = (LbmObservables * max(1, n)).from_address(self._mem.data_ptr())
+        self._n = n
+
+    def __len__(self) -> int:
+        return self._n
+
+    def address(self, i: int) -> int:
+        return self._mem.data_ptr() + i * C.sizeof(LbmObservables)
+
+    def __getitem__(self, i: int) -> dict:
+        if not 0 <= i < self._n:
+            raise IndexError(i)
+        return self._recs[i].as_dict()
+
+
 class Case:
     """One Rayleigh–Bénard case resident in HBM (src/globals.cu's device
     arrays, owned by this object instead of process globals)."""
@@ -369,6 +393,15 @@ class Case:
         if rc != OK and not (allow_diverged and rc == ERR_DIVERGED):
             check(rc)
         return [out[i].as_dict() for i in range(n)]
+
+    def step_observed_async(self, n: int, out: "ObservablesBuffer", first: int = 0, stream=None):
+        """Enqueue n steps and the copy of their observables into out[first ..
+        first + n) (C ABI lbm_step_observed_async) and return at once; the
+        entries are valid after the stream passes this call."""
+        if n < 0 or first < 0 or first + n > len(out):
+            raise ValueError("observables buffer too small")
+        check(lib().lbm_step_observed_async(self._h, int(n), C.c_void_p(out.address(first)),
+                                            _stream_handle(stream)))
 
     @property
     def step_kernel(self) -> int:

@@ -830,7 +830,8 @@ int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
     return LBM_OK;
 }
 
-int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream) {
+// lbm_step_observed (wait = true) and lbm_step_observed_async (false).
+static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream, bool wait) {
     int rc = check_mutable(c, true);
     if (rc) return rc;
     if (nsteps < 0) return fail(LBM_ERR_ARG, "nsteps < 0");
@@ -890,12 +891,21 @@ int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *s
     if (rc) return rc;
     c->step += nsteps;
     CUDA_TRY(cudaGetLastError());
-    CUDA_TRY(cudaMemcpyAsync(out, c->obs_series, (size_t)nsteps * sizeof(lbm_observables), cudaMemcpyDeviceToHost,
-                             st));
+    // in stream order before the next call's kernels rewrite obs_series
+    CUDA_TRY(cudaMemcpyAsync(out, c->obs_series, (size_t)nsteps * sizeof(lbm_observables), cudaMemcpyDefault, st));
+    if (!wait) return LBM_OK;
     CUDA_TRY(cudaStreamSynchronize(st));
     for (int s = 0; s < nsteps; s++)
         if (out[s].diverged) return fail(LBM_ERR_DIVERGED, "NaN/Inf in the macroscopic fields");
     return LBM_OK;
+}
+
+int lbm_step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream) {
+    return step_observed(c, nsteps, out, stream, true);
+}
+
+int lbm_step_observed_async(lbm_case *c, int32_t nsteps, lbm_observables *out, void *stream) {
+    return step_observed(c, nsteps, out, stream, false);
 }
 
 int lbm_get_profile(lbm_case *c, double *out, void *stream) {

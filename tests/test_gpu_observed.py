@@ -82,3 +82,50 @@ def test_step_observed_rules(lbm):
         c.set_step_kernel(lbm.KERNEL_ROW)
         with pytest.raises(lbm.LbmError):
             c.step_observed(1)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s"])
+def test_step_observed_async_matches_blocking(lbm, storage):
+    """lbm_step_observed_async enqueues the same steps and copies: the
+    records equal lbm_step_observed's bit for bit once the stream has
+    passed the calls, in chunks of 1 and 3 steps."""
+    import torch
+
+    p = lbm.make_params(24, 20, 16, rayleigh=1e6, storage=storage, sides=lbm.SIDES_PERIODIC)
+    stream = torch.cuda.Stream()
+    buf = lbm.ObservablesBuffer(10)
+    with lbm.Case(p) as a, lbm.Case(p) as b:
+        for c in (a, b):
+            c.init_conduction(5, 1e-2)
+            c.step(20)
+        want = b.step_observed(4) + b.step_observed(6)
+        for i in range(4):
+            a.step_observed_async(1, buf, first=i, stream=stream)
+        a.step_observed_async(3, buf, first=4, stream=stream)
+        a.step_observed_async(3, buf, first=7, stream=stream)
+        stream.synchronize()
+        got = [buf[i] for i in range(10)]
+        assert got == want
+        assert a.observables() == b.observables()
+
+
+def test_step_observed_async_rules(lbm):
+    p = lbm.make_params(32, 8, 8, storage="f32", sides=lbm.SIDES_PERIODIC)
+    buf = lbm.ObservablesBuffer(2)
+    with lbm.Case(p) as c:
+        with pytest.raises(lbm.LbmError):
+            c.step_observed_async(1, buf)   # not initialised
+        c.init_conduction(1)
+        with pytest.raises(ValueError):
+            c.step_observed_async(3, buf)
+        with pytest.raises(ValueError):
+            c.step_observed_async(1, buf, first=2)
+        c.step_observed_async(2, buf)
+        c.step_observed_async(0, buf)
+        c.set_step_kernel(lbm.KERNEL_ROW)
+        with pytest.raises(lbm.LbmError):
+            c.step_observed_async(1, buf)
+        import torch
+
+        torch.cuda.synchronize()
+        assert [buf[i]["step"] for i in range(2)] == [0, 1]
