@@ -433,6 +433,13 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
 
 template <class S, bool SW, bool PER, bool OBS = false>
 void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
+    // 16-bit storage, BGK: one node's update split over two warps
+    if constexpr (sizeof(S) == 2 && !OBS) {
+        if (c->collision == LBM_COLLISION_BGK) {
+            step16_split_kernel<S, SW, PER><<<grid_for(c->nodes, 64), 128, 0, st>>>(a);
+            return;
+        }
+    }
     const unsigned grid = grid_for(c->nodes, kStepThreads);
     if (c->collision == LBM_COLLISION_REGULARIZED)
         step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED, OBS><<<grid, kStepThreads, 0, st>>>(a);
