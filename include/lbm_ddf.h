@@ -59,7 +59,9 @@ extern "C" {
 
 /* step kernels (same results, different data movement) */
 #define LBM_KERNEL_AUTO 0      /* NODE (measured the fastest on B200) */
-#define LBM_KERNEL_NODE 1      /* one node per thread, any grid and side-wall mode */
+#define LBM_KERNEL_NODE 1      /* one node per thread, any grid and side-wall mode (16-bit
+                                  storage with BGK collision: each node's update split
+                                  over two warps, each taking half the populations) */
 #define LBM_KERNEL_ROW 2       /* whole x-rows staged by bulk copies; FP32 or FP64 storage,
                                   periodic sides, 32 <= LX <= 256, LX*element size a
                                   multiple of 16 bytes */
