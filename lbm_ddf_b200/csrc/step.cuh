@@ -782,6 +782,20 @@ __host__ __device__ constexpr int half_of(int k) {
                : 1;
 }
 
+// Every population in exactly one half, opposite pairs together (the
+// in-place update of a pair's two locations stays within one warp), 13 and
+// 14 populations.
+__host__ __device__ constexpr bool split_halves_ok() {
+    int n0 = 0;
+    for (int k = 0; k < Q; k++) {
+        if (half_of(k) != 0 && half_of(k) != 1) return false;
+        if (half_of(k) != half_of(opp(k))) return false;
+        n0 += half_of(k) == 0;
+    }
+    return n0 == 13 && half_of(0) == 0;
+}
+static_assert(split_halves_ok(), "split update: bad population halves");
+
 template <int H, class S, bool SWAPPED, bool INTERIOR, class A>
 __device__ __forceinline__ void gather_half(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
