@@ -93,8 +93,17 @@ def test_case_bytes(lbm):
 
 
 def test_null_case_is_an_error(lbm):
-    assert lbm.lib().lbm_step(None, 1, None) == lbm.ERR_ARG
-    assert lbm.lib().lbm_destroy(None) == lbm.OK
+    L = lbm.lib()
+    assert L.lbm_step(None, 1, None) == lbm.ERR_ARG
+    assert L.lbm_destroy(None) == lbm.OK
+    out = (lbm.LbmObservables * 2)()
+    assert L.lbm_step_observed(None, 1, out, None) == lbm.ERR_ARG
+    assert L.lbm_step_observed_async(None, 1, C.cast(out, C.c_void_p), None) == lbm.ERR_ARG
+    t = np.zeros(8, dtype=np.float32)
+    assert L.lbm_init_temperature(None, t.ctypes.data_as(C.c_void_p), None) == lbm.ERR_ARG
+    assert L.lbm_init_conduction(None, 1, 1e-3, None) == lbm.ERR_ARG
+    assert L.lbm_get_observables(None, C.byref(out[0]), None) == lbm.ERR_ARG
+    assert "NULL" in L.lbm_last_error().decode()
 
 
 def test_fastdiv_host_emulation():
