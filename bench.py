@@ -1,10 +1,12 @@
 """Benchmark of the fused LBM-DDF time step on B200.
 
-Workload (default): one Rayleigh–Bénard case of 256^3 nodes, Ra = 1e7,
-Pr = 0.71, free-fall velocity 0.1, hot/cold plates, periodic sides, seeded
-conduction start, FP32 populations.  A "step" is one fused time step of the
-whole grid (one kernel launch).  The state (3.6 GB) is larger than L2, so no
-flush is needed between steps.
+Headline workload (both arms): one Rayleigh–Bénard case of 256^3 nodes,
+Ra = 1e7, Pr = 0.71, free-fall velocity 0.1, hot/cold plates, closed side
+walls (the reference program's only mode), FP64 populations (the reference's
+only precision), starting from the seeded conduction state (seed 1000, noise
+1e-3).  A "step" is one fused time step of the whole grid (one kernel
+launch).  The state (7.3 GB) is larger than L2, so no flush is needed
+between steps.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
 
@@ -25,16 +27,21 @@ engine arm (default): prints one JSON line with
              at the end (host<->device copies of the full state);
   roofline   algorithmic bytes per launch (f and g read once and written
              once: 2*27*2 words per node) over the measured launch time,
-             against the measured HBM copy bandwidth;
-  cpu_baseline  the CPU oracle (OpenMP, FP64, reference operation order) on a
-             bounded 64^3 sample on this host's cores (rank 0, N = 1 only).
+             against the measured HBM copy bandwidth, and the DRAM bytes per
+             launch ncu measured (profiles/step_traffic.json);
+  companions the same measurements (value, e2e, roofline) for the
+             configuration's periodic sides in FP64, FP32, FP16S and BF16S;
+  cpu_baseline  the CPU oracle (OpenMP; the FP64 checker, and the same
+             transcription built in FP32) on a bounded 64^3 sample on this
+             host's cores (rank 0, N = 1 only).
 Under torchrun every rank advances its own independent case (replicas: the
 path needs no exchange between GPUs), so scaling is weak.
 
 reference arm: the reference's own program (Summer536/LBM_DDF src/, rebuilt
-unchanged for sm_100a by oracle/build_ref.py; FP64, closed box — the only mode
-it has) on the same grid; its per-step GPU time comes from the CUDA-event
-timing it prints, differenced between a 3-step and a longer run.
+unchanged for sm_100a by oracle/build_ref.py), fed the same seeded 256^3
+state through its restart path (src/initial.cu:110-205); its per-step GPU
+time is the difference of the CUDA-event time it prints for a 203-step and a
+3-step run, over 200 steps.
 """
 from __future__ import annotations
 
@@ -51,6 +58,13 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 FALLBACK_HBM_GBS = 6650.0
+METRIC = "MLUPS (fused LBM-DDF D3Q27 f+g step) & %HBM peak"
+SEED = 1000          # seed of rank 0's case; the reference arm's state uses it too
+AMPLITUDE = 1e-3
+GRID = 256
+RAYLEIGH, PRANDTL = 1e7, 0.71
+HEADLINE = ("f64", "wall")
+COMPANIONS = [("f64", "periodic"), ("f32", "periodic"), ("f16s", "periodic"), ("bf16s", "periodic")]
 
 
 def measured_hbm():
@@ -60,6 +74,14 @@ def measured_hbm():
             return float(json.load(fh)["hbm_gbs"]), "measured"
     except Exception:
         return FALLBACK_HBM_GBS, "fallback"
+
+
+def workload_config(grid: int, storage: str, sides: str) -> dict:
+    """The `config` of a line; the reference arm prints the same one."""
+    box = "closed box (the reference's side walls)" if sides == "wall" else "periodic sides"
+    return {"workload": f"RB {grid}x{grid}x{grid} Ra={RAYLEIGH:.0e} Pr={PRANDTL} {box}, seeded conduction start "
+                        f"(seed {SEED}, noise {AMPLITUDE:g}), {storage} populations",
+            "nodes_per_gpu": grid ** 3, "l2": "state larger than L2 (no flush needed)"}
 
 
 class ClockSampler:
@@ -122,7 +144,7 @@ class ClockSampler:
 def dist_setup(backend: str = "nccl"):
     """One process per GPU (torchrun's RANK / WORLD_SIZE / LOCAL_RANK).  The
     ranks are independent replicas; the process group carries only the
-    barriers around the timed region and the max over ranks of its time.
+    barriers around the timed regions and the max over ranks of their times.
     backend "gloo" runs the same plumbing on CPU (tests)."""
     import datetime
 
@@ -161,28 +183,38 @@ def barrier(world: int):
         dist.barrier()
 
 
-def workload(args):
-    return dict(lx=args.grid, ly=args.grid, lz=args.grid, rayleigh=1e7, prandtl=0.71)
-
-
-def cpu_baseline(seconds: float = 15.0):
-    """Oracle (OpenMP, FP64) on a bounded 64^3 sample of the same problem."""
+def cpu_baseline(seconds: float = 10.0, sides: str = "wall"):
+    """The oracle (OpenMP) on a bounded 64^3 sample of the same problem: the
+    FP64 checker (the reference's operation order) and the same
+    transcription built in FP32."""
     from oracle import oracle as orc
 
-    o = orc.Oracle(orc.make_params(64, 64, 64, rayleigh=1e5, periodic_sides=True))
-    o.init_conduction(1, 1e-3)
-    o.step(1)  # warm-up
-    steps = 0
-    t0 = time.perf_counter()
-    while True:
-        o.step(1)
-        steps += 1
-        dt = time.perf_counter() - t0
-        if dt >= seconds or steps >= 2000:
-            break
-    mlups = o.n * steps / dt / 1e6
-    return {"value": round(mlups, 3), "unit": "MLUPS", "cores": orc.threads(), "kind": "port",
-            "sample": f"64^3 periodic, FP64 oracle step (reference operation order, OpenMP), {steps} steps in {dt:.1f} s"}
+    def run(precision):
+        o = orc.Oracle(orc.make_params(64, 64, 64, rayleigh=1e5, periodic_sides=sides == "periodic"),
+                       precision=precision)
+        o.init_conduction(SEED, AMPLITUDE)
+        o.step(1)  # warm-up
+        steps = 0
+        t0 = time.perf_counter()
+        while True:
+            o.step(1)
+            steps += 1
+            dt = time.perf_counter() - t0
+            if dt >= seconds or steps >= 2000:
+                break
+        n = o.n
+        o.close()
+        return n * steps / dt / 1e6, steps, dt
+
+    box = "closed box" if sides == "wall" else "periodic sides"
+    v64, s64, d64 = run("f64")
+    v32, s32, d32 = run("f32")
+    return {"value": round(v64, 3), "unit": "MLUPS", "cores": orc.threads(), "kind": "port",
+            "sample": f"64^3 {box}, Ra 1e5, FP64 oracle step (reference operation order, OpenMP), "
+                      f"{s64} steps in {d64:.1f} s",
+            "f32": {"value": round(v32, 3), "unit": "MLUPS", "cores": orc.threads(), "kind": "port",
+                    "sample": f"64^3 {box}, Ra 1e5, the same transcription built in FP32 (OpenMP), "
+                              f"{s32} steps in {d32:.1f} s"}}
 
 
 def time_steps(case, stream, steps: int):
@@ -198,47 +230,60 @@ def time_steps(case, stream, steps: int):
     return start.elapsed_time(end) / 1e3
 
 
-def run_engine(args):
+def traffic_per_launch(storage: str, sides: str, grid: int):
+    """DRAM bytes (read + write) per step launch that ncu measured for this
+    storage, side-wall mode and grid (profiles/step_traffic.json), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "step_traffic.json")) as fh:
+            tr = json.load(fh).get(f"{storage}_{sides}", {}).get(str(grid))
+        return None if tr is None else float(tr)
+    except Exception:
+        return None
+
+
+def measure(lbm, args, storage: str, sides: str, rank: int, world: int, dev: int, stream, kind: int,
+            resume: bool = False, clocks: bool = False) -> dict:
+    """Device-timed steps, the end-to-end new run (and resumed run) and the
+    roofline of one configuration; every rank takes the same steps."""
     import numpy as np
     import torch
 
-    import lbm_ddf_b200 as lbm
-
-    rank, world, local = dist_setup()
-    dev = local if world > 1 else 0
-    torch.cuda.set_device(dev)
-    w = workload(args)
-    p = lbm.make_params(w["lx"], w["ly"], w["lz"], rayleigh=w["rayleigh"], prandtl=w["prandtl"],
-                        sides=lbm.SIDES_PERIODIC, storage=args.storage, device=dev)
-    nodes = w["lx"] * w["ly"] * w["lz"]
-    stream = torch.cuda.Stream(device=dev)
+    g = args.grid
+    p = lbm.make_params(g, g, g, rayleigh=RAYLEIGH, prandtl=PRANDTL,
+                        sides=lbm.SIDES_WALL if sides == "wall" else lbm.SIDES_PERIODIC, storage=storage, device=dev)
+    nodes = g ** 3
     bytes_per_lu = 2 * 27 * 2 * lbm.STORAGE_BYTES[p.storage]
+    seed = SEED + rank
+    out = {}
 
-    kind = {"auto": lbm.KERNEL_AUTO, "node": lbm.KERNEL_NODE, "row": lbm.KERNEL_ROW}[args.kernel]
     case = lbm.Case(p)
     case.set_step_kernel(kind)
-    kernel_used = {lbm.KERNEL_NODE: "node", lbm.KERNEL_ROW: "row"}[case.step_kernel]
-    case.init_conduction(1000 + rank, 1e-3, stream=stream)
+    out["step_kernel"] = {lbm.KERNEL_NODE: "node", lbm.KERNEL_ROW: "row"}[case.step_kernel]
+    case.init_conduction(seed, AMPLITUDE, stream=stream)
     case.step(args.warmup, stream=stream)
     torch.cuda.synchronize()
     barrier(world)
-    with ClockSampler(torch.cuda.current_device()) as clk:
+    if clocks:
+        with ClockSampler(torch.cuda.current_device()) as clk:
+            secs = time_steps(case, stream, args.steps)
+        out["clocks"] = clk.summary()
+    else:
         secs = time_steps(case, stream, args.steps)
     barrier(world)
     secs = max_over_ranks(secs, world)
-    clocks = clk.summary()
-    obs = case.observables(stream=stream)
-    ms_per_step = secs / args.steps * 1e3
-    value = world * nodes * args.steps / secs / 1e6
+    out["observables"] = {k: v for k, v in case.observables(stream=stream).items()
+                          if k in ("step", "nu_bulk", "nu_top", "nu_bottom", "ke", "re")}
+    out["value"] = round(world * nodes * args.steps / secs / 1e6, 2)
+    out["ms_per_step"] = round(secs / args.steps * 1e3, 4)
+    peak, peak_src = measured_hbm()
+    achieved = bytes_per_lu * nodes / (secs / args.steps) / 1e9
+    out["roofline"] = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                       "frac": round(achieved / peak, 4), "traffic": traffic_per_launch(storage, sides, g),
+                       "algorithmic_bytes_per_lu": bytes_per_lu, "peak_source": peak_src}
 
-    # Two whole jobs through the public API with host buffers, each: input
-    # from pinned host memory -> K x (step, observables of its start state to
-    # the host) -> observables of the final state.
-    #   e2e         a new run: the seeded conduction temperature field (made
-    #               on the host, outside the timed region) copied in by
-    #               init_temperature, populations at equilibrium from it;
-    #   e2e_resume  a resumed run: the whole state restored from a host
-    #               checkpoint, and saved back to it at the end.
+    # Whole jobs through the public API with host buffers, each: input from
+    # pinned host memory -> K x (step, observables of its start state to the
+    # host) -> observables of the final state.
     fused = kind != lbm.KERNEL_ROW
     obs_buf = lbm.ObservablesBuffer(args.steps)
     events = [torch.cuda.Event(), torch.cuda.Event()]
@@ -263,8 +308,7 @@ def run_engine(args):
 
     obs_bytes = ctypes.sizeof(lbm.LbmObservables) * (args.steps + (1 if fused else 0)) // args.steps
     tdtype = np.float64 if p.storage == lbm.STORE_F64 else np.float32
-    temp = torch.from_numpy(lbm.conduction_temperature(w["lx"], w["ly"], w["lz"], 1000 + rank, 1e-3,
-                                                       dtype=tdtype)).pin_memory()
+    temp = torch.from_numpy(lbm.conduction_temperature(g, g, g, seed, AMPLITUDE, dtype=tdtype)).pin_memory()
     e2e_case = lbm.Case(p)
     e2e_case.set_step_kernel(kind)
     # untimed warm-up job: first launches of the observed-step kernels and
@@ -278,110 +322,104 @@ def run_engine(args):
     job_steps(e2e_case)
     stream.synchronize()
     e2e_secs = max_over_ranks(time.perf_counter() - t0, world)
-    e2e_value = world * nodes * args.steps / e2e_secs / 1e6
-    temp_bytes = temp.numel() * temp.element_size()
     e2e_case.close()
+    out["e2e"] = {"value": round(world * nodes * args.steps / e2e_secs / 1e6, 2), "unit": "MLUPS",
+                  "h2d_bytes_per_step": int(temp.numel() * temp.element_size() / args.steps),
+                  "d2h_bytes_per_step": obs_bytes,
+                  "what": "new run: seeded temperature field from pinned host memory (init_temperature: "
+                          "equilibrium populations), K x (step + observables of its start state to pinned host "
+                          "memory, read by the host one step later"
+                          + (", reduced in the step kernel" if fused and lbm.STORAGE_BYTES[p.storage] > 2 else "")
+                          + "), observables of the final state"}
     del temp
 
-    nbytes = case.checkpoint_bytes()
-    host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
-    case.save_state(host, stream=stream)
-    torch.cuda.synchronize()
-    res_case = lbm.Case(p)
-    res_case.set_step_kernel(kind)
-    res_case.restore_state(host, stream=stream)
-    job_steps(res_case, min(args.warmup, args.steps))
-    stream.synchronize()
-    barrier(world)
-    t0 = time.perf_counter()
-    res_case.restore_state(host, stream=stream)
-    job_steps(res_case)
-    res_case.save_state(host, stream=stream)
-    stream.synchronize()
-    res_secs = max_over_ranks(time.perf_counter() - t0, world)
-    res_value = world * nodes * args.steps / res_secs / 1e6
-    res_case.close()
-    del host
-
-    # FP64 companion measurement (same workload, FP64 populations)
-    f64 = None
-    if args.storage != "f64" and not args.no_f64:
+    if resume:
+        nbytes = case.checkpoint_bytes()
+        host = torch.empty(nbytes, dtype=torch.uint8, pin_memory=True)
+        case.save_state(host, stream=stream)
+        torch.cuda.synchronize()
         case.close()
-        p64 = lbm.make_params(w["lx"], w["ly"], w["lz"], rayleigh=w["rayleigh"], prandtl=w["prandtl"],
-                              sides=lbm.SIDES_PERIODIC, storage="f64", device=dev)
-        c64 = lbm.Case(p64)
-        c64.set_step_kernel(kind)
-        c64.init_conduction(1000 + rank, 1e-3, stream=stream)
-        c64.step(args.warmup, stream=stream)
+        res_case = lbm.Case(p)
+        res_case.set_step_kernel(kind)
+        res_case.restore_state(host, stream=stream)
+        job_steps(res_case, min(args.warmup, args.steps))
+        stream.synchronize()
         barrier(world)
-        s64 = max_over_ranks(time_steps(c64, stream, args.steps), world)
-        c64.close()
-        peak, src = measured_hbm()
-        ach = 2 * 27 * 2 * 8 * nodes / (s64 / args.steps) / 1e9
-        f64 = {"value": round(world * nodes * args.steps / s64 / 1e6, 2), "ms_per_step": round(s64 / args.steps * 1e3, 4),
-               "roofline_frac": round(ach / peak, 4), "achieved_gbs": round(ach, 1)}
+        t0 = time.perf_counter()
+        res_case.restore_state(host, stream=stream)
+        job_steps(res_case)
+        res_case.save_state(host, stream=stream)
+        stream.synchronize()
+        res_secs = max_over_ranks(time.perf_counter() - t0, world)
+        res_case.close()
+        del host
+        out["e2e_resume"] = {"value": round(world * nodes * args.steps / res_secs / 1e6, 2), "unit": "MLUPS",
+                             "h2d_bytes_per_step": int(nbytes / args.steps),
+                             "d2h_bytes_per_step": int(nbytes / args.steps) + obs_bytes,
+                             "what": "resumed run: whole state restored from a pinned host checkpoint, K x (step "
+                                     "+ observables to host), observables of the final state, state saved to host"}
     else:
         case.close()
+    return out
 
+
+def run_engine(args):
+    import torch
+
+    import lbm_ddf_b200 as lbm
+
+    rank, world, local = dist_setup()
+    dev = local if world > 1 else 0
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream(device=dev)
+    kind = {"auto": lbm.KERNEL_AUTO, "node": lbm.KERNEL_NODE, "row": lbm.KERNEL_ROW}[args.kernel]
+    if kind == lbm.KERNEL_ROW and args.sides == "wall":
+        raise SystemExit("the row-staged kernel runs periodic sides only: pass --sides periodic")
+    head = measure(lbm, args, args.storage, args.sides, rank, world, dev, stream, kind, resume=True, clocks=True)
+    companions = {}
+    if not args.no_companions:
+        for st, sd in COMPANIONS:
+            if (st, sd) == (args.storage, args.sides):
+                continue
+            k = kind if (kind != lbm.KERNEL_ROW or st in ("f32", "f64")) else lbm.KERNEL_NODE
+            m = measure(lbm, args, st, sd, rank, world, dev, stream, k)
+            companions[f"{st}_{sd}"] = {"config": workload_config(args.grid, st, sd),
+                                        **{x: m[x] for x in ("value", "ms_per_step", "e2e", "roofline",
+                                                             "step_kernel")}}
     if world > 1:
         import torch.distributed as dist
 
         dist.destroy_process_group()
     if rank != 0:
         return 0
-    peak, peak_src = measured_hbm()
-    achieved = bytes_per_lu * nodes / (secs / args.steps) / 1e9
-    traffic = None
-    tpath = os.path.join(ROOT, "profiles", "step_traffic.json")
-    try:
-        with open(tpath) as fh:
-            tr = json.load(fh).get(args.storage, {}).get(str(args.grid))
-            traffic = tr if tr is None else float(tr)
-    except Exception:
-        traffic = None
     line = {
-        "metric": "MLUPS (fused LBM-DDF D3Q27 f+g step) & %HBM peak",
-        "value": round(value, 2),
+        "metric": METRIC,
+        "value": head["value"],
         "unit": "MLUPS",
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": round(ms_per_step, 4),
+        "ms_per_step": head["ms_per_step"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "f32" if args.storage != "f64" else "f64",
+        "dtype": "f64" if args.storage == "f64" else "f32",
         "storage": args.storage,
         "data": "synthetic (seeded conduction profile + 1e-3 noise)",
-        "config": {"workload": f"RB {w['lx']}x{w['ly']}x{w['lz']} Ra={w['rayleigh']:.0e} Pr={w['prandtl']} "
-                               f"periodic sides, {args.storage} populations",
-                   "nodes_per_gpu": nodes, "l2": "state larger than L2 (no flush needed)",
-                   "step_kernel": kernel_used,
-                   "parallelism": f"replicas x{world}"},
-        "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
-                "h2d_bytes_per_step": int(temp_bytes / args.steps),
-                "d2h_bytes_per_step": obs_bytes,
-                "what": "new run: seeded temperature field from pinned host memory (init_temperature: "
-                        "equilibrium populations), K x (step + observables of its start state to pinned host "
-                        "memory, read by the host one step later"
-                        + (", reduced in the step kernel" if fused and lbm.STORAGE_BYTES[p.storage] > 2 else "")
-                        + "), observables of the final state"},
-        "e2e_resume": {"value": round(res_value, 2), "unit": "MLUPS",
-                       "h2d_bytes_per_step": int(nbytes / args.steps),
-                       "d2h_bytes_per_step": int(nbytes / args.steps) + obs_bytes,
-                       "what": "resumed run: whole state restored from a pinned host checkpoint, K x (step + "
-                               "observables to host), observables of the final state, state saved to host"},
-        "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                     "frac": round(achieved / peak, 4), "traffic": traffic,
-                     "algorithmic_bytes_per_lu": bytes_per_lu, "peak_source": peak_src},
+        "config": workload_config(args.grid, args.storage, args.sides),
+        "parallelism": f"replicas x{world}",
+        "step_kernel": head["step_kernel"],
+        "e2e": head["e2e"],
+        "e2e_resume": head["e2e_resume"],
+        "roofline": head["roofline"],
         "gpu_launches": args.steps,
-        "clocks": clocks,
-        "observables": {k: obs[k] for k in ("step", "nu_bulk", "nu_top", "nu_bottom", "ke", "re")},
+        "clocks": head["clocks"],
+        "observables": head["observables"],
     }
-    if f64 is not None:
-        line["f64"] = f64
+    if companions:
+        line["companions"] = companions
     if world == 1 and not args.no_cpu:
-        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds)
+        line["cpu_baseline"] = cpu_baseline(args.cpu_seconds, args.sides)
     print(json.dumps(line), flush=True)
     return 0
 
@@ -392,39 +430,46 @@ def run_reference(args):
     if rank != 0:
         return 0
     from oracle import ref_run
-    from oracle.ref_cases import REF_CASES, TIMING_SETS
+    from oracle.ref_cases import REF_CASES, TIMING_SEED, TIMING_SETS
 
+    def unavailable(why):
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        return 0
+
+    if args.storage != "f64" or args.sides != "wall":
+        return unavailable("the reference runs FP64 populations in a closed box only")
     tag = {256: "c1", 64: "c0"}.get(args.grid)
     if tag is None:
-        print(json.dumps({"impl": "reference", "unavailable": f"no reference build for grid {args.grid}"}))
-        return 0
-    short, longs = TIMING_SETS[tag]
-    longer = min(longs, key=lambda n: abs((n - short) - args.steps))
-    a, b = f"{tag}_n{short}", f"{tag}_n{longer}"
-    if not (os.path.exists(ref_run.binary(a)) and os.path.exists(ref_run.binary(b))):
-        print(json.dumps({"impl": "reference", "unavailable": "reference binaries not built (oracle/build_ref.py)"}))
-        return 0
-    c = REF_CASES[b]
+        return unavailable(f"no reference build for grid {args.grid}")
+    short, long_ = TIMING_SETS[tag]
+    if not (os.path.exists(ref_run.binary(short)) and os.path.exists(ref_run.binary(long_))):
+        return unavailable("reference binaries not built (oracle/build_ref.py)")
+    c = REF_CASES[long_]
     nodes = c["lx"] * c["ly"] * c["lz"]
-    ta = ref_run.time_case(a)
+    assert TIMING_SEED == SEED
+    state = ref_run.conduction_restart(c["lx"], c["ly"], c["lz"], TIMING_SEED, AMPLITUDE)
+    ta = ref_run.time_case(short, restart=state)
     with ClockSampler(0) as clk:
-        tb = ref_run.time_case(b)
-    steps = longer - short
+        tb = ref_run.time_case(long_, restart=state)
+    steps = REF_CASES[long_]["nend"] - REF_CASES[short]["nend"]
     per_step = (tb - ta) / steps
     value = nodes / per_step / 1e6
     line = {
         "impl": "reference",
-        "metric": "MLUPS (fused LBM-DDF D3Q27 f+g step) & %HBM peak",
-        "value": round(value, 2), "unit": "MLUPS", "n_gpus": 1, "steps": steps, "warmup": short,
+        "metric": METRIC,
+        "value": round(value, 2), "unit": "MLUPS", "n_gpus": 1, "steps": steps,
+        "warmup": REF_CASES[short]["nend"] - REF_CASES[short]["continue_step"],
         "ms_per_step": round(per_step * 1e3, 4), "higher_is_better": True, "scaling": "weak",
-        "vs_baseline": None, "dtype": "f64", "data": "synthetic (reference rest state)",
-        "config": {"workload": f"RB {c['lx']}x{c['ly']}x{c['lz']} Ra={c['rayleigh']:.0e} Pr={c['prandtl']} "
-                               "closed box, f64 populations (the reference's only mode)",
-                   "nodes_per_gpu": nodes},
+        "vs_baseline": None, "dtype": "f64", "storage": "f64",
+        "data": "synthetic (seeded conduction profile + 1e-3 noise)",
+        "config": workload_config(args.grid, "f64", "wall"),
         "e2e": {"value": round(value, 2), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "cpu_baseline": {"value": round(value, 2), "unit": "MLUPS", "cores": 1, "kind": "reference",
-                         "sample": f"reference src/ built for sm_100a, GPU time it prints for {longer} vs {short} "
-                                   f"steps (2-decimal seconds), one host thread driving the GPU"},
+                         "sample": f"reference src/ built for sm_100a, fed the seeded state through its restart "
+                                   f"files; GPU time it prints (2 decimals, CUDA events per step) for "
+                                   f"{REF_CASES[long_]['nend'] - REF_CASES[long_]['continue_step']} vs "
+                                   f"{REF_CASES[short]['nend'] - REF_CASES[short]['continue_step']} steps, one host "
+                                   f"thread driving the GPU"},
         "clocks": clk.summary(),
         "ran_on": "GPU (the reference is CUDA only; it has no CPU implementation)",
         "world_size_requested": world,
@@ -439,12 +484,13 @@ def parse_args(argv=None):
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--grid", type=int, default=256)
-    ap.add_argument("--storage", default="f32", choices=["f64", "f32", "f16s", "bf16s"])
+    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--storage", default=HEADLINE[0], choices=["f64", "f32", "f16s", "bf16s"])
+    ap.add_argument("--sides", default=HEADLINE[1], choices=["wall", "periodic"])
     ap.add_argument("--kernel", default="auto", choices=["auto", "node", "row"])
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--no-f64", action="store_true")
-    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--no-companions", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
     args = ap.parse_args(argv)
     if args.warmup < 3:
         args.warmup = 3

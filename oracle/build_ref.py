@@ -22,7 +22,10 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, "_ref")
-REF_SRC = os.environ.get("LBM_REFERENCE_SRC", "/root/reference/src")
+# The reference's src/ directory: LBM_REFERENCE_SRC, else a checkout of the
+# reference project beside this repository (../reference/src).
+REF_SRC = os.environ.get("LBM_REFERENCE_SRC") or os.path.normpath(
+    os.path.join(HERE, "..", "..", "reference", "src"))
 SOURCES = ["main.cu", "globals.cu", "initial.cu", "collision.cu", "streaming.cu",
            "macrovar.cu", "output.cu"]
 NEVER = 1_000_000_000

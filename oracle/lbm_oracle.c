@@ -20,6 +20,13 @@
 #include <omp.h>
 #endif
 
+/* State and step arithmetic: orc_real (lbm_oracle.h) is double, the
+ * reference's precision, unless the library is built with -DORC_REAL=float
+ * (oracle/Makefile's liblbm_oracle_f32.so, which also makes unsuffixed
+ * constants float): the same transcription in FP32, the CPU baseline of the
+ * FP32 engine.  Parameters, the noise and the diagnostics' sums stay double. */
+typedef orc_real real;
+
 /* D3Q27 velocity set in the reference's population order, src/initial.cu:71-73. */
 static const int CX[ORC_Q] = {0, 1, 0, -1, 0, 0, 0, 1, -1, -1, 1, 1, 0, -1,
                               0, 1, 0, -1, 0, 1, -1, -1, 1, 1, -1, -1, 1};
@@ -54,22 +61,22 @@ void orc_set_contract(int mask) { orc_contract = mask; }
 int orc_get_contract(void) { return orc_contract; }
 
 /* a*b + c, fused (one rounding) when the site's bit is set */
-static inline double mad(int site, double a, double b, double c) {
-    return (orc_contract & site) ? fma(a, b, c) : a * b + c;
+static inline real mad(int site, real a, real b, real c) {
+    return (orc_contract & site) ? _Generic(a, float: fmaf, default: fma)(a, b, c) : a * b + c;
 }
 
 struct orc_state {
     orc_params p;
     int64_t n;
-    double *f, *g, *f_temp, *g_temp;
-    double *rho, *ux, *uy, *uz, *phi, *fx, *fy, *fz;
-    double w[ORC_Q];
+    real *f, *g, *f_temp, *g_temp;
+    real *rho, *ux, *uy, *uz, *phi, *fx, *fy, *fz;
+    real w[ORC_Q];
     int opp[ORC_Q];
     int collision;          /* ORC_COLLISION_BGK (the reference) or _REGULARIZED */
 };
 
 /* Lattice weights, src/initial.cu:77-83. */
-static void orc_weights(double *w) {
+static void orc_weights(real *w) {
     for (int i = 0; i < ORC_Q; i++) {
         if (i == 0)
             w[i] = 8.0 / 27.0;
@@ -116,20 +123,20 @@ orc_state *orc_create(const orc_params *p) {
     if (!s) return NULL;
     s->p = q;
     s->n = (int64_t)q.lx * q.ly * q.lz;
-    size_t big = (size_t)ORC_Q * (size_t)s->n * sizeof(double);
-    size_t one = (size_t)s->n * sizeof(double);
-    s->f = (double *)calloc(1, big);
-    s->g = (double *)calloc(1, big);
-    s->f_temp = (double *)calloc(1, big);
-    s->g_temp = (double *)calloc(1, big);
-    s->rho = (double *)calloc(1, one);
-    s->ux = (double *)calloc(1, one);
-    s->uy = (double *)calloc(1, one);
-    s->uz = (double *)calloc(1, one);
-    s->phi = (double *)calloc(1, one);
-    s->fx = (double *)calloc(1, one);
-    s->fy = (double *)calloc(1, one);
-    s->fz = (double *)calloc(1, one);
+    size_t big = (size_t)ORC_Q * (size_t)s->n * sizeof(real);
+    size_t one = (size_t)s->n * sizeof(real);
+    s->f = (real *)calloc(1, big);
+    s->g = (real *)calloc(1, big);
+    s->f_temp = (real *)calloc(1, big);
+    s->g_temp = (real *)calloc(1, big);
+    s->rho = (real *)calloc(1, one);
+    s->ux = (real *)calloc(1, one);
+    s->uy = (real *)calloc(1, one);
+    s->uz = (real *)calloc(1, one);
+    s->phi = (real *)calloc(1, one);
+    s->fx = (real *)calloc(1, one);
+    s->fy = (real *)calloc(1, one);
+    s->fz = (real *)calloc(1, one);
     if (!s->f || !s->g || !s->f_temp || !s->g_temp || !s->rho || !s->ux || !s->uy || !s->uz ||
         !s->phi || !s->fx || !s->fy || !s->fz) {
         orc_destroy(s);
@@ -151,7 +158,7 @@ void orc_destroy(orc_state *s) {
 const orc_params *orc_get_params(const orc_state *s) { return &s->p; }
 int64_t orc_nodes(const orc_state *s) { return s->n; }
 
-double *orc_field(orc_state *s, int which) {
+real *orc_field(orc_state *s, int which) {
     switch (which) {
     case 0: return s->f;
     case 1: return s->g;
@@ -171,7 +178,7 @@ double *orc_field(orc_state *s, int which) {
 
 /* src/macrovar.cu:36-47 */
 static void k_forcing(orc_state *s) {
-    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    const real gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
     const int64_t n = s->n;
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < n; i++) {
@@ -183,25 +190,25 @@ static void k_forcing(orc_state *s) {
 
 /* src/collision.cu:3-33 (lines 34-49 compute a stress tensor that is discarded). */
 static void k_collide_f(orc_state *s) {
-    const double tau = s->p.tau;
+    const real tau = s->p.tau;
     const int64_t n = s->n;
-    double *f = s->f;
+    real *f = s->f;
 #pragma omp parallel for schedule(static)
     for (int64_t idx = 0; idx < n; idx++) {
-        double fy9 = s->fy[idx];
-        double rho9 = s->rho[idx];
-        double u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
+        real fy9 = s->fy[idx];
+        real rho9 = s->rho[idx];
+        real u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
         for (int ip = 0; ip < ORC_Q; ip++) {
-            double RT = 1.0 / 3.0;
+            real RT = 1.0 / 3.0;
             /* c*u products are exact (c in {-1,0,1}), so fusing them changes nothing */
-            double eu = ((double)CX[ip] * u9 + (double)CY[ip] * v9 + (double)CZ[ip] * w9) / RT;
-            double uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;  /* (u*u + v*v + w*w) / RT */
-            double q = mad(FUSE_Q_F, eu, eu, -uv);                   /* eu*eu - uv */
-            double feq_in = rho9 + eu + 0.5 * q;
+            real eu = ((real)CX[ip] * u9 + (real)CY[ip] * v9 + (real)CZ[ip] * w9) / RT;
+            real uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;  /* (u*u + v*v + w*w) / RT */
+            real q = mad(FUSE_Q_F, eu, eu, -uv);                   /* eu*eu - uv */
+            real feq_in = rho9 + eu + 0.5 * q;
             /* -(f - w*feq_in) / tau, the product fused into the subtraction */
-            double fchange = -mad(FUSE_FEQ, -s->w[ip], feq_in, f[ip * n + idx]) / tau;
-            double feq_rho0 = s->w[ip] * (1.0 + eu + 0.5 * q);
-            double fc = (1.0 - 0.5 / tau) * fy9 * ((double)CY[ip] - v9) / RT;
+            real fchange = -mad(FUSE_FEQ, -s->w[ip], feq_in, f[ip * n + idx]) / tau;
+            real feq_rho0 = s->w[ip] * (1.0 + eu + 0.5 * q);
+            real fc = (1.0 - 0.5 / tau) * fy9 * ((real)CY[ip] - v9) / RT;
             fchange = mad(FUSE_FORCE, fc, feq_rho0, fchange);        /* fchange += fc * feq_rho0 */
             f[ip * n + idx] += fchange;
         }
@@ -210,21 +217,21 @@ static void k_collide_f(orc_state *s) {
 
 /* src/collision.cu:52-64 */
 static void k_collide_g(orc_state *s) {
-    const double tauc = s->p.tauc;
+    const real tauc = s->p.tauc;
     const int64_t n = s->n;
-    double *g = s->g;
+    real *g = s->g;
 #pragma omp parallel for schedule(static)
     for (int64_t idx = 0; idx < n; idx++) {
-        double phi9 = s->phi[idx];
-        double u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
-        double RT = 1.0 / 3.0;
+        real phi9 = s->phi[idx];
+        real u9 = s->ux[idx], v9 = s->uy[idx], w9 = s->uz[idx];
+        real RT = 1.0 / 3.0;
         for (int ip = 0; ip < ORC_Q; ip++) {
-            double g9 = g[ip * n + idx];
-            double eu = ((double)CX[ip] * u9 + (double)CY[ip] * v9 + (double)CZ[ip] * w9) / RT;
-            double uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;
-            double geq_in = 1.0 + eu + 0.5 * mad(FUSE_Q_G, eu, eu, -uv);
+            real g9 = g[ip * n + idx];
+            real eu = ((real)CX[ip] * u9 + (real)CY[ip] * v9 + (real)CZ[ip] * w9) / RT;
+            real uv = mad(FUSE_UV, w9, w9, mad(FUSE_UV, u9, u9, v9 * v9)) / RT;
+            real geq_in = 1.0 + eu + 0.5 * mad(FUSE_Q_G, eu, eu, -uv);
             /* -(g9 - (w*phi9)*geq_in) / tauc, the product fused into the subtraction */
-            double gchange = -mad(FUSE_GEQ, -(s->w[ip] * phi9), geq_in, g9) / tauc;
+            real gchange = -mad(FUSE_GEQ, -(s->w[ip] * phi9), geq_in, g9) / tauc;
             g[ip * n + idx] += gchange;
         }
     }
@@ -244,62 +251,62 @@ static void k_collide_g(orc_state *s) {
  *   g_i <- geq_i + (1 - 1/tau_c) gneq_i.
  * Mass, momentum and phi are those of BGK; at tau = 1 both are feq + force. */
 static void k_collide_f_reg(orc_state *s) {
-    const double tau = s->p.tau;
-    const double keep = 1.0 - 1.0 / tau, force_fac = 1.0 - 0.5 / tau;
+    const real tau = s->p.tau;
+    const real keep = 1.0 - 1.0 / tau, force_fac = 1.0 - 0.5 / tau;
     const int64_t n = s->n;
-    double *f = s->f;
+    real *f = s->f;
 #pragma omp parallel for schedule(static)
     for (int64_t idx = 0; idx < n; idx++) {
-        const double fy = s->fy[idx], rho = s->rho[idx];
-        const double u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
-        const double uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-        double m2[3][3] = {{0}};
+        const real fy = s->fy[idx], rho = s->rho[idx];
+        const real u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
+        const real uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        real m2[3][3] = {{0}};
         for (int ip = 0; ip < ORC_Q; ip++) {
             const int c[3] = {CX[ip], CY[ip], CZ[ip]};
-            const double fi = f[ip * n + idx];
+            const real fi = f[ip * n + idx];
             for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) m2[a][b] += (double)(c[a] * c[b]) * fi;
+                for (int b = 0; b < 3; b++) m2[a][b] += (real)(c[a] * c[b]) * fi;
         }
-        double pi[3][3];
+        real pi[3][3];
         for (int a = 0; a < 3; a++)
             for (int b = 0; b < 3; b++) pi[a][b] = m2[a][b] - (a == b ? rho / 3.0 : 0.0) - u[a] * u[b];
-        const double tr3 = (pi[0][0] + pi[1][1] + pi[2][2]) / 3.0;
+        const real tr3 = (pi[0][0] + pi[1][1] + pi[2][2]) / 3.0;
         for (int ip = 0; ip < ORC_Q; ip++) {
             const int c[3] = {CX[ip], CY[ip], CZ[ip]};
-            const double eu = 3.0 * (c[0] * u[0] + c[1] * u[1] + c[2] * u[2]);
-            const double p = eu + 0.5 * (eu * eu - uv);
-            const double feq = s->w[ip] * (rho + p);
-            const double feq0 = s->w[ip] * (1.0 + p);
-            double qpi = -tr3;
+            const real eu = 3.0 * (c[0] * u[0] + c[1] * u[1] + c[2] * u[2]);
+            const real p = eu + 0.5 * (eu * eu - uv);
+            const real feq = s->w[ip] * (rho + p);
+            const real feq0 = s->w[ip] * (1.0 + p);
+            real qpi = -tr3;
             for (int a = 0; a < 3; a++)
-                for (int b = 0; b < 3; b++) qpi += (double)(c[a] * c[b]) * pi[a][b];
-            const double fneq = 4.5 * s->w[ip] * qpi;
-            const double fc = force_fac * fy * ((double)c[1] - u[1]) * 3.0;
+                for (int b = 0; b < 3; b++) qpi += (real)(c[a] * c[b]) * pi[a][b];
+            const real fneq = 4.5 * s->w[ip] * qpi;
+            const real fc = force_fac * fy * ((real)c[1] - u[1]) * 3.0;
             f[ip * n + idx] = feq + keep * fneq + fc * feq0;
         }
     }
 }
 
 static void k_collide_g_reg(orc_state *s) {
-    const double keep = 1.0 - 1.0 / s->p.tauc;
+    const real keep = 1.0 - 1.0 / s->p.tauc;
     const int64_t n = s->n;
-    double *g = s->g;
+    real *g = s->g;
 #pragma omp parallel for schedule(static)
     for (int64_t idx = 0; idx < n; idx++) {
-        const double phi = s->phi[idx];
-        const double u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
-        const double uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-        double j[3] = {-phi * u[0], -phi * u[1], -phi * u[2]};
+        const real phi = s->phi[idx];
+        const real u[3] = {s->ux[idx], s->uy[idx], s->uz[idx]};
+        const real uv = 3.0 * (u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+        real j[3] = {-phi * u[0], -phi * u[1], -phi * u[2]};
         for (int ip = 0; ip < ORC_Q; ip++) {
-            const double gi = g[ip * n + idx];
-            j[0] += (double)CX[ip] * gi;
-            j[1] += (double)CY[ip] * gi;
-            j[2] += (double)CZ[ip] * gi;
+            const real gi = g[ip * n + idx];
+            j[0] += (real)CX[ip] * gi;
+            j[1] += (real)CY[ip] * gi;
+            j[2] += (real)CZ[ip] * gi;
         }
         for (int ip = 0; ip < ORC_Q; ip++) {
-            const double eu = 3.0 * (CX[ip] * u[0] + CY[ip] * u[1] + CZ[ip] * u[2]);
-            const double geq = s->w[ip] * phi * (1.0 + eu + 0.5 * (eu * eu - uv));
-            const double gneq = 3.0 * s->w[ip] * (CX[ip] * j[0] + CY[ip] * j[1] + CZ[ip] * j[2]);
+            const real eu = 3.0 * (CX[ip] * u[0] + CY[ip] * u[1] + CZ[ip] * u[2]);
+            const real geq = s->w[ip] * phi * (1.0 + eu + 0.5 * (eu * eu - uv));
+            const real gneq = 3.0 * s->w[ip] * (CX[ip] * j[0] + CY[ip] * j[1] + CZ[ip] * j[2]);
             g[ip * n + idx] = geq + keep * gneq;
         }
     }
@@ -324,9 +331,9 @@ static void k_stream(orc_state *s, int scalar) {
     const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
     const int per = s->p.periodic_sides;
     const int64_t n = s->n;
-    const double *src = scalar ? s->g : s->f;
-    double *dst = scalar ? s->g_temp : s->f_temp;
-    const double t_hot = s->p.t_hot, t_cold = s->p.t_cold;
+    const real *src = scalar ? s->g : s->f;
+    real *dst = scalar ? s->g_temp : s->f_temp;
+    const real t_hot = s->p.t_hot, t_cold = s->p.t_cold;
 #pragma omp parallel for schedule(static)
     for (int iz = 0; iz < lz; iz++) {
         for (int iy = 0; iy < ly; iy++) {
@@ -348,10 +355,10 @@ static void k_stream(orc_state *s, int scalar) {
                         dst[k * n + idx] = src[k * n + sidx];
                         continue;
                     }
-                    double back = src[(int64_t)s->opp[k] * n + idx];
+                    real back = src[(int64_t)s->opp[k] * n + idx];
                     if (scalar && out_y && !out_z) {
-                        double density = s->rho[idx];
-                        double tw = (sy < 0) ? t_hot : t_cold;
+                        real density = s->rho[idx];
+                        real tw = (sy < 0) ? t_hot : t_cold;
                         dst[k * n + idx] = mad(FUSE_ABB, 2.0 * s->w[k] * tw, 1.0 + density, -back);
                     } else {
                         dst[k * n + idx] = back;
@@ -367,14 +374,14 @@ static void k_macrovar(orc_state *s) {
     const int64_t n = s->n;
 #pragma omp parallel for schedule(static)
     for (int64_t idx = 0; idx < n; idx++) {
-        double rho_l = 0.0, ux_l = 0.0, uy_l = 0.0, uz_l = 0.0, phi_l = 0.0;
+        real rho_l = 0.0, ux_l = 0.0, uy_l = 0.0, uz_l = 0.0, phi_l = 0.0;
         for (int ip = 0; ip < ORC_Q; ip++) {
-            double f_val = s->f[ip * n + idx];
-            double g_val = s->g[ip * n + idx];
+            real f_val = s->f[ip * n + idx];
+            real g_val = s->g[ip * n + idx];
             rho_l += f_val;
-            ux_l += (double)CX[ip] * f_val;
-            uy_l += (double)CY[ip] * f_val;
-            uz_l += (double)CZ[ip] * f_val;
+            ux_l += (real)CX[ip] * f_val;
+            uy_l += (real)CY[ip] * f_val;
+            uz_l += (real)CZ[ip] * f_val;
             phi_l += g_val;
         }
         s->rho[idx] = rho_l;
@@ -386,7 +393,7 @@ static void k_macrovar(orc_state *s) {
 }
 
 void orc_step(orc_state *s, int nsteps) {
-    size_t bytes = (size_t)ORC_Q * (size_t)s->n * sizeof(double);
+    size_t bytes = (size_t)ORC_Q * (size_t)s->n * sizeof(real);
     for (int it = 0; it < nsteps; it++) {
         k_forcing(s);          /* src/main.cu:27 */
         if (s->collision == ORC_COLLISION_REGULARIZED) {
@@ -409,7 +416,7 @@ void orc_step(orc_state *s, int nsteps) {
 /* src/initial.cu:208-241 */
 void orc_init_rest(orc_state *s) {
     const int64_t n = s->n;
-    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    const real gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
     for (int64_t idx = 0; idx < n; idx++) {
         s->rho[idx] = 0.0;
         s->ux[idx] = 0.0;
@@ -419,11 +426,11 @@ void orc_init_rest(orc_state *s) {
         s->fx[idx] = 0.0;
         s->fy[idx] = gb * (s->phi[idx] - t0);
         s->fz[idx] = 0.0;
-        double usq = 0.0;
+        real usq = 0.0;
         for (int ip = 0; ip < ORC_Q; ip++) {
-            double feq = s->w[ip] * s->rho[idx] * (1.0 - 1.5 * usq);
-            s->f[ip * n + idx] = feq - 0.5 * s->fy[idx] * (double)CY[ip] / (1.0 / 3.0) * feq;
-            double geq = s->w[ip] * s->phi[idx] * (1.0 - 1.5 * usq);
+            real feq = s->w[ip] * s->rho[idx] * (1.0 - 1.5 * usq);
+            s->f[ip * n + idx] = feq - 0.5 * s->fy[idx] * (real)CY[ip] / (1.0 / 3.0) * feq;
+            real geq = s->w[ip] * s->phi[idx] * (1.0 - 1.5 * usq);
             s->g[ip * n + idx] = geq;
         }
     }
@@ -442,13 +449,13 @@ double orc_noise_uniform(uint64_t seed, uint64_t node) {
     return (double)(r >> 11) * (1.0 / 9007199254740992.0);
 }
 
-void orc_set_populations(orc_state *s, const double *f, const double *g, const double *phi_prev) {
+void orc_set_populations(orc_state *s, const real *f, const real *g, const real *phi_prev) {
     const int64_t n = s->n;
-    const double gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
-    memcpy(s->f, f, (size_t)ORC_Q * (size_t)n * sizeof(double));
-    memcpy(s->g, g, (size_t)ORC_Q * (size_t)n * sizeof(double));
+    const real gb = s->p.gravity * s->p.beta, t0 = s->p.t0;
+    memcpy(s->f, f, (size_t)ORC_Q * (size_t)n * sizeof(real));
+    memcpy(s->g, g, (size_t)ORC_Q * (size_t)n * sizeof(real));
     for (int64_t i = 0; i < n; i++) {
-        double pp = phi_prev ? phi_prev[i] : t0;
+        real pp = phi_prev ? phi_prev[i] : t0;
         s->fx[i] = 0.0;
         s->fy[i] = gb * (pp - t0);
         s->fz[i] = 0.0;
@@ -459,9 +466,9 @@ void orc_set_populations(orc_state *s, const double *f, const double *g, const d
 void orc_init_conduction(orc_state *s, uint64_t seed, double amplitude) {
     const int lx = s->p.lx, ly = s->p.ly, lz = s->p.lz;
     const int64_t n = s->n;
-    double *f = (double *)calloc((size_t)ORC_Q * (size_t)n, sizeof(double));
-    double *g = (double *)malloc((size_t)ORC_Q * (size_t)n * sizeof(double));
-    double *pp = (double *)malloc((size_t)n * sizeof(double));
+    real *f = (real *)calloc((size_t)ORC_Q * (size_t)n, sizeof(real));
+    real *g = (real *)malloc((size_t)ORC_Q * (size_t)n * sizeof(real));
+    real *pp = (real *)malloc((size_t)n * sizeof(real));
     if (!f || !g || !pp) {
         free(f); free(g); free(pp);
         return;
@@ -482,9 +489,9 @@ void orc_init_conduction(orc_state *s, uint64_t seed, double amplitude) {
 
 /* src/initial.cu:110-205: the restart reader copies all seven arrays, then
  * launches forcing (:202). */
-void orc_load_restart(orc_state *s, const double *rho, const double *ux, const double *uy,
-                      const double *uz, const double *phi, const double *f, const double *g) {
-    const size_t one = (size_t)s->n * sizeof(double);
+void orc_load_restart(orc_state *s, const real *rho, const real *ux, const real *uy,
+                      const real *uz, const real *phi, const real *f, const real *g) {
+    const size_t one = (size_t)s->n * sizeof(real);
     memcpy(s->rho, rho, one);
     memcpy(s->ux, ux, one);
     memcpy(s->uy, uy, one);
@@ -511,7 +518,7 @@ void orc_observables(const orc_state *s, double out[10]) {
     int64_t cnt = 0;
     for (int ix = 0; ix < lx; ix++)
         for (int iz = 0; iz < lz; iz++) {
-            const double *p = s->phi;
+            const real *p = s->phi;
             int64_t b0 = ((int64_t)iz * ly + 0) * lx + ix;
             int64_t b1 = ((int64_t)iz * ly + 1) * lx + ix;
             int64_t b2 = ((int64_t)iz * ly + 2) * lx + ix;

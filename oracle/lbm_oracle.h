@@ -29,6 +29,15 @@ extern "C" {
 
 #define ORC_Q 27
 
+/* Type of the populations, macroscopic fields and step arithmetic: double
+ * (the reference's FP64; this build is pinned bitwise to its outputs), or
+ * float when built with -DORC_REAL=float (liblbm_oracle_f32.so: the same
+ * transcription in FP32, a CPU baseline only). */
+#ifndef ORC_REAL
+#define ORC_REAL double
+#endif
+typedef ORC_REAL orc_real;
+
 typedef struct orc_params {
     int32_t lx, ly, lz;          /* LX, LY, LZ of src/parameters.h:8-10 */
     int32_t periodic_sides;      /* 0 = closed box (reference), 1 = x and z periodic */
@@ -44,7 +53,7 @@ typedef struct orc_state orc_state;
 /* Derived parameters, src/globals.cu:13-23. Returns 0, or -1 on a bad grid. */
 int orc_derive(orc_params *p);
 
-/* Allocates the reference's 4x27 + 8 FP64 fields (src/initial.cu:5-18). */
+/* Allocates the reference's 4x27 + 8 fields (src/initial.cu:5-18). */
 orc_state *orc_create(const orc_params *p);
 void orc_destroy(orc_state *s);
 const orc_params *orc_get_params(const orc_state *s);
@@ -52,7 +61,7 @@ int64_t orc_nodes(const orc_state *s);
 
 /* Field pointers (reference layout, length N or 27*N). which: 0 f, 1 g,
  * 2 rho, 3 ux, 4 uy, 5 uz, 6 phi, 7 force_x, 8 force_y, 9 force_z. */
-double *orc_field(orc_state *s, int which);
+orc_real *orc_field(orc_state *s, int which);
 
 /* Rest state of init_arrays, src/initial.cu:208-241. */
 void orc_init_rest(orc_state *s);
@@ -73,14 +82,14 @@ double orc_noise_uniform(uint64_t seed, uint64_t node);
  * would leave them after a step whose force was built from phi_prev:
  *   F_y = g*beta*(phi_prev - t0), rho = sum f, u = sum c f + F/2, phi = sum g.
  * phi_prev == NULL means phi_prev = t0 (zero force). */
-void orc_set_populations(orc_state *s, const double *f, const double *g,
-                         const double *phi_prev);
+void orc_set_populations(orc_state *s, const orc_real *f, const orc_real *g,
+                         const orc_real *phi_prev);
 
 /* Restart path (src/initial.cu:110-205): copies rho, ux, uy, uz, phi, f, g
  * verbatim and then runs `forcing` (src/initial.cu:202). */
-void orc_load_restart(orc_state *s, const double *rho, const double *ux,
-                      const double *uy, const double *uz, const double *phi,
-                      const double *f, const double *g);
+void orc_load_restart(orc_state *s, const orc_real *rho, const orc_real *ux,
+                      const orc_real *uy, const orc_real *uz, const orc_real *phi,
+                      const orc_real *f, const orc_real *g);
 
 /* nsteps time steps of src/main.cu:27-46:
  * forcing -> collision_BGK -> collision_BGK_scalar -> streaming (+copy)

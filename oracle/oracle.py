@@ -5,7 +5,9 @@ TEST INFRASTRUCTURE ONLY: the parity tests, ``__graft_entry__.smoke()`` and
 The product package ``lbm_ddf_b200`` never imports it.
 
 The oracle restates the reference single-GPU step (Summer536/LBM_DDF ``src/``)
-in FP64; see ``oracle/lbm_oracle.h`` for the per-function citations.
+in FP64; see ``oracle/lbm_oracle.h`` for the per-function citations.  The
+same transcription compiled in FP32 (``precision="f32"``,
+liblbm_oracle_f32.so) is only a CPU baseline for bench.py, not a checker.
 """
 from __future__ import annotations
 
@@ -17,6 +19,9 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "liblbm_oracle.so")
+LIB_PATHS = {"f64": LIB_PATH, "f32": os.path.join(HERE, "liblbm_oracle_f32.so")}
+CTYPES = {"f64": C.c_double, "f32": C.c_float}
+DTYPES = {"f64": np.float64, "f32": np.float32}
 
 Q = 27
 # D3Q27 order of src/initial.cu:71-73
@@ -38,7 +43,7 @@ class OrcParams(C.Structure):
     ]
 
 
-_lib = None
+_libs = {}
 
 
 def build() -> str:
@@ -47,14 +52,14 @@ def build() -> str:
     return LIB_PATH
 
 
-def lib():
-    global _lib
-    if _lib is None:
-        if not os.path.exists(LIB_PATH):
+def lib(precision: str = "f64"):
+    if precision not in _libs:
+        if not os.path.exists(LIB_PATHS[precision]):
             build()
-        L = C.CDLL(LIB_PATH)
+        L = C.CDLL(LIB_PATHS[precision])
         P = C.POINTER(OrcParams)
         dp = C.POINTER(C.c_double)
+        rp = C.POINTER(CTYPES[precision])
         L.orc_derive.argtypes = [P]
         L.orc_derive.restype = C.c_int
         L.orc_create.argtypes = [P]
@@ -63,13 +68,13 @@ def lib():
         L.orc_nodes.argtypes = [C.c_void_p]
         L.orc_nodes.restype = C.c_int64
         L.orc_field.argtypes = [C.c_void_p, C.c_int]
-        L.orc_field.restype = dp
+        L.orc_field.restype = rp
         L.orc_init_rest.argtypes = [C.c_void_p]
         L.orc_init_conduction.argtypes = [C.c_void_p, C.c_uint64, C.c_double]
         L.orc_noise_uniform.argtypes = [C.c_uint64, C.c_uint64]
         L.orc_noise_uniform.restype = C.c_double
-        L.orc_set_populations.argtypes = [C.c_void_p, dp, dp, dp]
-        L.orc_load_restart.argtypes = [C.c_void_p] + [dp] * 7
+        L.orc_set_populations.argtypes = [C.c_void_p, rp, rp, rp]
+        L.orc_load_restart.argtypes = [C.c_void_p] + [rp] * 7
         L.orc_step.argtypes = [C.c_void_p, C.c_int]
         L.orc_observables.argtypes = [C.c_void_p, dp]
         L.orc_profile.argtypes = [C.c_void_p, dp]
@@ -78,8 +83,8 @@ def lib():
         L.orc_set_collision.argtypes = [C.c_void_p, C.c_int]
         L.orc_get_collision.argtypes = [C.c_void_p]
         L.orc_get_contract.restype = C.c_int
-        _lib = L
-    return _lib
+        _libs[precision] = L
+    return _libs[precision]
 
 
 def _dp(a: np.ndarray):
@@ -109,19 +114,22 @@ COLLISIONS = {"bgk": 0, "regularized": 1}
 
 
 class Oracle:
-    """One reference-layout FP64 case on the CPU."""
+    """One reference-layout case on the CPU: FP64 (the checker) or, with
+    precision="f32", the FP32 build of the same transcription."""
 
-    def __init__(self, params: OrcParams):
+    def __init__(self, params: OrcParams, precision: str = "f64"):
         self.params = params
-        self._h = lib().orc_create(C.byref(params))
+        self.precision = precision
+        self._L = lib(precision)
+        self._h = self._L.orc_create(C.byref(params))
         if not self._h:
             raise MemoryError("orc_create failed")
-        self.n = int(lib().orc_nodes(self._h))
+        self.n = int(self._L.orc_nodes(self._h))
         self.shape = (params.lz, params.ly, params.lx)
 
     def close(self):
-        if self._h:
-            lib().orc_destroy(self._h)
+        if getattr(self, "_h", None):
+            self._L.orc_destroy(self._h)
             self._h = None
 
     def __del__(self):
@@ -129,49 +137,55 @@ class Oracle:
 
     def field(self, name: str) -> np.ndarray:
         """Live numpy view of a field (f and g are (27, LZ, LY, LX))."""
-        ptr = lib().orc_field(self._h, FIELDS[name])
+        ptr = self._L.orc_field(self._h, FIELDS[name])
         count = self.n * (Q if name in ("f", "g") else 1)
         a = np.ctypeslib.as_array(ptr, shape=(count,))
         return a.reshape((Q,) + self.shape if name in ("f", "g") else self.shape)
 
+    def _rp(self, a):
+        a = np.ascontiguousarray(a, dtype=DTYPES[self.precision])
+        return a, a.ctypes.data_as(C.POINTER(CTYPES[self.precision]))
+
     def init_rest(self):
-        lib().orc_init_rest(self._h)
+        self._L.orc_init_rest(self._h)
 
     def init_conduction(self, seed: int, amplitude: float = 1e-3):
-        lib().orc_init_conduction(self._h, C.c_uint64(seed), amplitude)
+        self._L.orc_init_conduction(self._h, C.c_uint64(seed), amplitude)
 
     def set_populations(self, f, g, phi_prev=None):
-        f = np.ascontiguousarray(f, dtype=np.float64)
-        g = np.ascontiguousarray(g, dtype=np.float64)
-        pp = None if phi_prev is None else _dp(np.ascontiguousarray(phi_prev, dtype=np.float64))
-        lib().orc_set_populations(self._h, _dp(f), _dp(g), pp)
+        f, fp = self._rp(f)
+        g, gp = self._rp(g)
+        pp = None
+        if phi_prev is not None:
+            phi_prev, pp = self._rp(phi_prev)
+        self._L.orc_set_populations(self._h, fp, gp, pp)
 
     def load_restart(self, rho, ux, uy, uz, phi, f, g):
-        arrs = [np.ascontiguousarray(a, dtype=np.float64) for a in (rho, ux, uy, uz, phi, f, g)]
-        lib().orc_load_restart(self._h, *[_dp(a) for a in arrs])
+        arrs = [self._rp(a) for a in (rho, ux, uy, uz, phi, f, g)]
+        self._L.orc_load_restart(self._h, *[p for _, p in arrs])
 
     def step(self, n: int = 1):
-        lib().orc_step(self._h, int(n))
+        self._L.orc_step(self._h, int(n))
 
     def set_collision(self, model: str):
         """'bgk' (the reference's) or 'regularized' (Latt and Chopard 2006)."""
-        lib().orc_set_collision(self._h, COLLISIONS[model])
+        self._L.orc_set_collision(self._h, COLLISIONS[model])
 
     @property
     def collision(self) -> str:
-        code = lib().orc_get_collision(self._h)
+        code = self._L.orc_get_collision(self._h)
         return next(k for k, v in COLLISIONS.items() if v == code)
 
     def observables(self) -> dict:
         out = np.zeros(10)
-        lib().orc_observables(self._h, _dp(out))
+        self._L.orc_observables(self._h, _dp(out))
         keys = ["nu_bulk", "nu_top", "nu_bottom", "ke", "re", "ux_mean", "uy_mean",
                 "uz_mean", "phi_mean", "diverged"]
         return dict(zip(keys, out.tolist()))
 
     def profile(self) -> np.ndarray:
         out = np.zeros(5 * self.params.ly)
-        lib().orc_profile(self._h, _dp(out))
+        self._L.orc_profile(self._h, _dp(out))
         return out.reshape(self.params.ly, 5)
 
 

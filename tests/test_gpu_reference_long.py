@@ -58,3 +58,25 @@ def test_f64_engine_equals_reference_program_10000_steps(lbm, oracle_mod):
     assert want.shape == (len(nu), 5)
     assert list(want[:, 0]) == [float(m) for m in marks]
     np.testing.assert_allclose(np.array(nu), want[:, 2:], rtol=2e-6, atol=1e-20)
+
+
+def test_reference_timing_runs_fed_through_pipes():
+    """bench.py's reference arm feeds the seeded conduction state to the
+    reference program through named pipes in place of its restart files
+    (src/initial.cu:110-205 reads them with sequential fread); at 64^3 both
+    timing runs complete and report a GPU time that grows with the steps."""
+    import torch
+
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from oracle import ref_run
+    from oracle.ref_cases import REF_CASES, TIMING_SEED, TIMING_SETS
+
+    short, long_ = TIMING_SETS["c0"]
+    if not (os.path.exists(ref_run.binary(short)) and os.path.exists(ref_run.binary(long_))):
+        pytest.skip("reference timing binaries not built")
+    c = REF_CASES[long_]
+    state = ref_run.conduction_restart(c["lx"], c["ly"], c["lz"], TIMING_SEED, 1e-3)
+    ta = ref_run.time_case(short, restart=state, timeout=300)
+    tb = ref_run.time_case(long_, restart=state, timeout=300)
+    assert 0.0 <= ta < tb

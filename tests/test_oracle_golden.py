@@ -115,3 +115,23 @@ def test_contraction_model_is_needed(oracle_mod):
         assert relerr(o.field("g").reshape(-1), g["g"].reshape(-1)) < 1e-15
     finally:
         oracle_mod.set_contract(default)
+
+
+@pytest.mark.parametrize("grid,seed", [((12, 10, 8), 20240611), ((16, 12, 10), 1000), ((8, 5, 4), 7)])
+def test_conduction_restart_bytes_match_oracle(oracle_mod, grid, seed):
+    """oracle/ref_run.conduction_restart (the restart files that feed the
+    reference program the seeded conduction state, in bench.py's reference
+    arm) is bitwise the oracle's own orc_init_conduction state."""
+    import numpy as np
+
+    from oracle.ref_run import conduction_restart
+
+    lx, ly, lz = grid
+    o = oracle_mod.Oracle(oracle_mod.make_params(lx, ly, lz, rayleigh=1e7))
+    o.init_conduction(seed, 1e-3)
+    flow, fg = conduction_restart(lx, ly, lz, seed, 1e-3)
+    want_flow = b"".join(o.field(k).reshape(-1).tobytes() for k in ("rho", "ux", "uy", "uz", "phi"))
+    want_fg = o.field("f").reshape(-1).tobytes() + o.field("g").reshape(-1).tobytes()
+    o.close()
+    assert b"".join(flow()) == want_flow
+    assert b"".join(fg()) == want_fg

@@ -9,6 +9,7 @@ oracle/lbm_oracle.c) that hold at any size, checked on the CPU:
 The same properties are checked for the CUDA engine in the GPU tests.
 """
 import numpy as np
+import pytest
 
 
 def test_bgk_mass_conserved_closed_box(oracle_mod):
@@ -46,3 +47,26 @@ def test_xz_mirror_symmetry(oracle_mod):
     assert np.max(np.abs(fs - got_f)) <= 1e-12 * scale
     assert np.max(np.abs(got_phi.transpose(2, 1, 0) - got_phi)) <= 1e-12
 
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_fp32_build_tracks_fp64(oracle_mod, periodic):
+    """liblbm_oracle_f32.so (the FP32 CPU baseline) computes the same update
+    as the FP64 checker: after 200 steps from the same seeded state its
+    fields agree to FP32 rounding (5e-5 field-relative, the bound the FP32
+    engine is held to)."""
+    from helpers import relerr
+
+    p = oracle_mod.make_params(16, 12, 10, rayleigh=1e5, periodic_sides=periodic)
+    o64 = oracle_mod.Oracle(p)
+    o32 = oracle_mod.Oracle(p, precision="f32")
+    assert o32.field("f").dtype == np.float32
+    for o in (o64, o32):
+        o.init_conduction(5, 1e-2)
+        o.step(200)
+    for k in ("f", "g", "phi", "rho"):
+        e = relerr(o32.field(k), o64.field(k))
+        assert e <= 5e-5, (k, e)
+    assert abs(o32.observables()["nu_bulk"] - o64.observables()["nu_bulk"]) <= 1e-4 * abs(o64.observables()["nu_bulk"])
+    o64.close()
+    o32.close()
