@@ -14,7 +14,8 @@ import hashlib
 import numpy as np
 import pytest
 
-from helpers import load_golden, nu_from_fields, relerr
+from helpers import (load_golden, nu_from_fields, relerr, shear_amplitude, shear_params, shear_state,
+                     shear_steps)
 from oracle.ref_cases import REF_CASES
 
 pytestmark = pytest.mark.gpu
@@ -357,6 +358,44 @@ def test_regularized_vs_oracle(lbm, oracle_mod, storage, tol, steps, periodic):
     compare(got, o, 1e-12 if storage == "f64" else 20 * tol, fields=("uy",))
     ob = o.observables()
     assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= (1e-10 if storage == "f64" else 50 * tol)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32"])
+@pytest.mark.parametrize("model", ["bgk", "regularized"])
+@pytest.mark.parametrize("tau", [0.51, 0.6, 1.0])
+def test_shear_wave_viscosity(lbm, oracle_mod, storage, model, tau):
+    """A decaying shear wave u_x(z) (periodic sides, plates far from the
+    mid-plane, no buoyancy) gives the engine's BGK and regularised
+    collisions the viscosity (tau - 1/2)/3 within 1% (the discretisation
+    error of a 32-node wave; tests/test_oracle_regularized.py shows it
+    shrinking with k), in FP64 and FP32 storage; the FP64 engine's measured
+    viscosity equals the oracle's to 1e-9."""
+    lx, ly, lz = 2, 48, 32
+    st = shear_state(lx, ly, lz)
+    p = lbm.make_params(lx, ly, lz, sides=lbm.SIDES_PERIODIC, storage=storage, **shear_params(tau, ly))
+    steps = shear_steps(tau, lz)
+    with lbm.Case(p) as c:
+        assert abs(c.derived["tau"] - tau) < 1e-12
+        c.set_collision(model)
+        c.load_ref_state(*(st[k] for k in ("rho", "ux", "uy", "uz", "phi", "f", "g")))
+        c.step(10)
+        a1 = shear_amplitude(c.store_ref_state(("ux",))["ux"], ly, lz)
+        c.step(steps)
+        a2 = shear_amplitude(c.store_ref_state(("ux",))["ux"], ly, lz)
+    k = 2.0 * np.pi / lz
+    nu = -np.log(a2 / a1) / (k * k * steps)
+    assert abs(nu / ((tau - 0.5) / 3.0) - 1.0) <= 1e-2, (storage, model, tau, nu)
+    if storage == "f64":
+        o = oracle_mod.Oracle(oracle_mod.make_params(lx, ly, lz, periodic_sides=True, **shear_params(tau, ly)))
+        o.set_collision(model)
+        o.load_restart(*(st[k] for k in ("rho", "ux", "uy", "uz", "phi", "f", "g")))
+        o.step(10)
+        b1 = shear_amplitude(o.field("ux"), ly, lz)
+        o.step(steps)
+        b2 = shear_amplitude(o.field("ux"), ly, lz)
+        o.close()
+        nu_o = -np.log(b2 / b1) / (k * k * steps)
+        assert abs(nu - nu_o) <= 1e-9 * nu_o, (nu, nu_o)
 
 
 def test_regularized_stays_stable_where_bgk_diverges(lbm):
