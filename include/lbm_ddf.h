@@ -200,15 +200,17 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
  *             number of steps from an init or load).  For F16S / BF16S the
  *             engine interleaves the two: one array of (f, g) pairs, row k
  *             at f + 2*k*pop_stride elements, node j's f at element 2j and
- *             its g at 2j + 1; pass g = f + 1 element;
+ *             its g at 2j + 1; g must be f + 1 element and pop_stride below
+ *             477,218,589 (nine rows of pairs are indexed in 32 bits), else
+ *             LBM_ERR_ARG; for F64 and F32, pop_stride is at most 2^40;
  *   phi_prev  previous-step temperature per node (double for F64, else float);
  *   out_dev   DEVICE memory for one lbm_observables, written on `stream`.
  * Enqueues two kernels on `stream` and returns without synchronising; the
  * caller reads out_dev after the stream.  The block partial sums go to a
  * fixed array inside the library (1184 rows of 13 doubles, 123 KB, held by
- * every GPU that loads the library until the process exits); it covers any
- * grid the C ABI accepts (fewer than 2^31 nodes) and calls needing more rows
- * are rejected with LBM_ERR_ARG.  Each call overwrites every row it reads,
+ * every GPU that loads the library until the process exits); the reduction
+ * never runs more than 1184 blocks, so the array covers every grid the C ABI
+ * accepts (fewer than 2^31 nodes).  Each call overwrites every row it reads,
  * so nothing has to be cleared between calls, but calls whose kernels
  * overlap on the GPU (other streams, other host threads) race on the array.
  * The first call on a device looks up the array's address; make that first
@@ -288,6 +290,16 @@ int lbm_batch_add(lbm_batch *b, lbm_case *c);
 int lbm_batch_remove(lbm_batch *b, lbm_case *c);
 int lbm_batch_size(const lbm_batch *b, int32_t *members, uint64_t *nodes);
 int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream);
+/* Observables of every member at its current step (as lbm_get_observables
+ * would report each), enqueued on `stream` into out[0 .. members) in the
+ * order the members were added (removals close the gaps), then returns
+ * without synchronising: out (page-locked host memory for an asynchronous
+ * copy, or device memory) is valid once the stream passes the call, and the
+ * caller checks out[i].diverged.  Call it on the stream the batch steps on,
+ * so it sees the steps enqueued before it.  It replaces one synchronising
+ * lbm_get_observables per member (the reference reduces its one case on the
+ * host, src/output.cu:148-280). */
+int lbm_batch_observables(lbm_batch *b, lbm_observables *out, void *stream);
 /* Launch shape: blocks of 128 or 256 threads, each tile 4 x block nodes of
  * one member; blocks_per_sm > 0 runs that many persistent blocks per SM
  * walking the tile list, 0 one block per tile; use_graph replays captured

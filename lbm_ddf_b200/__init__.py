@@ -115,6 +115,7 @@ def lib() -> C.CDLL:
         L.lbm_batch_remove.argtypes = [vp, vp]
         L.lbm_batch_size.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
         L.lbm_batch_step.argtypes = [vp, C.c_int32, vp]
+        L.lbm_batch_observables.argtypes = [vp, vp, vp]
         L.lbm_batch_set_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
         L.lbm_batch_get_config.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.lbm_batch_autotune.argtypes = [vp, C.c_int32, vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -129,7 +130,7 @@ def lib() -> C.CDLL:
                      "lbm_set_collision", "lbm_get_collision", "lbm_step_observed", "lbm_step_observed_async",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
-                     "lbm_batch_autotune"):
+                     "lbm_batch_autotune", "lbm_batch_observables"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -489,6 +490,27 @@ class Batch:
 
     def step(self, n: int = 1, stream=None):
         check(lib().lbm_batch_step(self._h, int(n), _stream_handle(stream)))
+
+    def observables_async(self, out: "ObservablesBuffer", stream=None):
+        """Enqueue the observables of every member, in self.members order,
+        into out[0 .. len(self.members)) (C ABI lbm_batch_observables) and
+        return at once; the entries are valid after the stream passes this
+        call (synchronise it or an event recorded after the call)."""
+        if len(out) < len(self.members):
+            raise ValueError("observables buffer too small")
+        check(lib().lbm_batch_observables(self._h, C.c_void_p(out.address(0)), _stream_handle(stream)))
+
+    def observables(self, stream=None) -> list:
+        """Observables of every member (self.members order); waits for the stream."""
+        import torch
+
+        out = ObservablesBuffer(len(self.members))
+        self.observables_async(out, stream)
+        if stream is None:
+            torch.cuda.synchronize()
+        else:
+            stream.synchronize()
+        return [out[i] for i in range(len(self.members))]
 
     def set_config(self, block: int = 128, blocks_per_sm: int = 0, use_graph: bool = True):
         check(lib().lbm_batch_set_config(self._h, block, blocks_per_sm, int(bool(use_graph))))

@@ -5,7 +5,9 @@
 // AA layout and collision model; one launch of batch_step_kernel per
 // non-empty group (normally one: members move through the layouts in step)
 // advances the group's members by one step.  Their nodes are cut into tiles
-// of kTileRounds x BLOCK nodes, numbered case after case; blocks walk the tile list with a
+// of kTileRounds x BLOCK nodes (x BLOCK / 2 for 16-bit BGK members, whose
+// node updates are split over two warps, batch_step16_split_kernel),
+// numbered case after case; blocks walk the tile list with a
 // grid stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block
 // per tile), find each tile's case by a binary search over the tiles' prefix
 // sums held in shared memory, and apply the same node update as the
@@ -28,7 +30,6 @@
 #include <vector>
 
 #include "internal.h"
-#include "step.cuh"
 #include "step.cuh"
 
 using namespace lbm;
@@ -117,6 +118,55 @@ __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
     }
 }
 
+// 16-bit storage, BGK: the members' node updates split over two warps, as in
+// the single-case step16_split_kernel (step.cuh split_update): warps 2p and
+// 2p + 1 of a block share 32 nodes, each loading, relaxing and storing half
+// of the populations.  A tile is kTileRounds rounds of BLOCK / 2 nodes of one
+// member.  A warp pair exchanges its partial moments once per round through
+// a two-buffer area (the partner reads round r's buffer before it reaches
+// the barrier of round r + 1, which the writer of round r + 2 has passed).
+// The tile prefix sums are in dynamic shared memory ((ncases + 1) words), so
+// kSplitBlocks blocks of 128 threads fit on an SM.
+template <int BLOCK> struct SplitBatchOccupancy {
+    static constexpr int value = kSplitBlocks * 128 / BLOCK;
+};
+
+template <class S, int BLOCK, bool SWAPPED>
+__global__ void __launch_bounds__(BLOCK, SplitBatchOccupancy<BLOCK>::value)
+    batch_step16_split_kernel(const BatchCase<S> *__restrict__ cases, int ncases,
+                              const uint32_t *__restrict__ tile_start) {
+    static_assert(BLOCK == 128 || BLOCK == 256, "two or four warp pairs");
+    extern __shared__ uint32_t s_start[];
+    __shared__ float xch[BLOCK / 64][2][2][5][32];   // [warp pair][buffer][half][moment][lane]
+    for (int i = threadIdx.x; i <= ncases; i += BLOCK) s_start[i] = tile_start[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int pair = warp >> 1;
+    constexpr uint32_t kRound = BLOCK / 2;            // nodes per round
+    const uint32_t end = s_start[ncases];
+    int buf = 0;
+    for (uint32_t t = s_start[0] + blockIdx.x; t < end; t += gridDim.x) {
+        int lo = 0, hi = ncases;   // the member c with s_start[c] <= t < s_start[c+1]
+        while (hi - lo > 1) {
+            const int mid = (lo + hi) >> 1;
+            if (s_start[mid] <= t) lo = mid;
+            else hi = mid;
+        }
+        const BatchCase<S> &cs = cases[lo];
+        const uint32_t u0 = (t - s_start[lo]) * (kRound * kTileRounds) + (uint32_t)(pair * 32 + lane);
+#pragma unroll 1
+        for (int r = 0; r < kTileRounds; r++) {
+            const uint32_t u = u0 + r * kRound;
+            const bool valid = u < cs.nodes;
+            if ((warp & 1) == 0)
+                split_update<0, S, SWAPPED, true>(cs, u, valid, xch[pair][buf], lane, pair);
+            else
+                split_update<1, S, SWAPPED, true>(cs, u, valid, xch[pair][buf], lane, pair);
+            buf ^= 1;
+        }
+    }
+}
+
 }  // namespace lbm
 
 struct lbm_batch {
@@ -138,6 +188,17 @@ struct lbm_batch {
     bool dirty = true;             // descriptors need rebuilding / uploading
     std::vector<unsigned char> h_cases;
     std::vector<uint32_t> h_start;
+    // page-locked staging of the descriptor uploads, two in turn: an upload
+    // is a copy on the step stream that needs no wait, and a staging buffer
+    // is reused only after its event says its copy is done
+    unsigned char *stage[2] = {nullptr, nullptr};
+    size_t stage_cap[2] = {0, 0};
+    cudaEvent_t stage_ev[2] = {nullptr, nullptr};
+    bool stage_used[2] = {false, false};
+    int stage_next = 0;
+    // lbm_batch_observables: one record per member (device)
+    lbm_observables *d_obs = nullptr;
+    int obs_cap = 0;
     // captured graphs, keyed by 2 x the number of steps + the phase at
     // capture; dropped when the membership or the launch shape changes
     std::map<int, cudaGraphExec_t> graphs;
@@ -209,6 +270,13 @@ int group_of(const lbm_batch *b, const lbm_case *c) {
     return ((c->swapped ? 1 : 0) ^ b->phase) | (c->collision == LBM_COLLISION_REGULARIZED ? 2 : 0);
 }
 
+// Nodes per tile of a member: kTileRounds rounds of the block's threads, or
+// of half of them where two warps share each node (16-bit BGK members).
+int64_t tile_nodes(const lbm_batch *b, const lbm_case *c) {
+    const bool split = interleaved(c) && c->collision == LBM_COLLISION_BGK;
+    return (int64_t)(split ? b->block / 2 : b->block) * kTileRounds;
+}
+
 // Rebuilds and uploads the descriptors after a membership change.
 int refresh(lbm_batch *b, cudaStream_t st) {
     if (!b->dirty) return LBM_OK;
@@ -249,7 +317,7 @@ int refresh(lbm_batch *b, cudaStream_t st) {
             const BatchCase<S> d = describe<S>(order[(size_t)i]);
             std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
             b->h_start[i] = tiles;
-            const int64_t tile = (int64_t)b->block * kTileRounds;
+            const int64_t tile = tile_nodes(b, order[(size_t)i]);
             tiles += (uint32_t)((order[(size_t)i]->nodes + tile - 1) / tile);
         }
         return LBM_OK;
@@ -257,11 +325,28 @@ int refresh(lbm_batch *b, cudaStream_t st) {
     if (rc) return rc;
     b->h_start[n] = tiles;
     if (n > 0) {
-        CUDA_TRY(cudaMemcpyAsync(b->d_cases, b->h_cases.data(), b->h_cases.size(), cudaMemcpyHostToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(b->d_start, b->h_start.data(), b->h_start.size() * sizeof(uint32_t),
-                                 cudaMemcpyHostToDevice, st));
-        // the host vectors must outlive the copies
-        CUDA_TRY(cudaStreamSynchronize(st));
+        // through page-locked staging: the copies run in stream order behind
+        // the steps already enqueued, and the host does not wait for them
+        const int i = b->stage_next;
+        const size_t cb = b->h_cases.size(), sb = b->h_start.size() * sizeof(uint32_t);
+        const size_t off = (cb + 255) / 256 * 256;
+        if (b->stage_used[i]) CUDA_TRY(cudaEventSynchronize(b->stage_ev[i]));
+        if (!b->stage_ev[i]) CUDA_TRY(cudaEventCreateWithFlags(&b->stage_ev[i], cudaEventDisableTiming));
+        if (b->stage_cap[i] < off + sb) {
+            if (b->stage[i]) cudaFreeHost(b->stage[i]);
+            b->stage[i] = nullptr;
+            b->stage_cap[i] = 0;
+            const size_t cap = std::max<size_t>(2 * (off + sb), 64 * 1024);
+            CUDA_TRY(cudaMallocHost((void **)&b->stage[i], cap));
+            b->stage_cap[i] = cap;
+        }
+        std::memcpy(b->stage[i], b->h_cases.data(), cb);
+        std::memcpy(b->stage[i] + off, b->h_start.data(), sb);
+        CUDA_TRY(cudaMemcpyAsync(b->d_cases, b->stage[i], cb, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(b->d_start, b->stage[i] + off, sb, cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaEventRecord(b->stage_ev[i], st));
+        b->stage_used[i] = true;
+        b->stage_next = 1 - i;
     }
     b->dirty = false;
     return LBM_OK;
@@ -274,8 +359,14 @@ unsigned grid_of(const lbm_batch *b, uint32_t tiles) {
 
 template <class S, int BLOCK, bool SW>
 void launch_group(const BatchCase<S> *cases, int n, const uint32_t *start, bool reg, unsigned grid, cudaStream_t st) {
-    if (reg) batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_REGULARIZED><<<grid, BLOCK, 0, st>>>(cases, n, start);
-    else batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
+    if (reg) {
+        batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_REGULARIZED><<<grid, BLOCK, 0, st>>>(cases, n, start);
+    } else if constexpr (sizeof(S) == 2) {   // 16-bit BGK: two warps per node
+        batch_step16_split_kernel<S, BLOCK, SW><<<grid, BLOCK, (size_t)(n + 1) * sizeof(uint32_t), st>>>(cases, n,
+                                                                                                        start);
+    } else {
+        batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
+    }
 }
 
 // Enqueues `nsteps` batch steps on `st`: per step one launch per non-empty
@@ -357,6 +448,14 @@ int lbm_batch_destroy(lbm_batch *b) {
     drop_graphs(b);
     cudaFree(b->d_cases);
     cudaFree(b->d_start);
+    cudaFree(b->d_obs);
+    for (int i = 0; i < 2; i++) {
+        if (b->stage_ev[i]) {
+            cudaEventSynchronize(b->stage_ev[i]);
+            cudaEventDestroy(b->stage_ev[i]);
+        }
+        if (b->stage[i]) cudaFreeHost(b->stage[i]);
+    }
     if (b->capture_stream) cudaStreamDestroy(b->capture_stream);
     delete b;
     return LBM_OK;
@@ -457,6 +556,39 @@ int lbm_batch_step(lbm_batch *b, int32_t nsteps, void *stream) {
         CUDA_TRY(cudaGetLastError());
     }
     advance_members(b, nsteps);
+    return LBM_OK;
+}
+
+int lbm_batch_observables(lbm_batch *b, lbm_observables *out, void *stream) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    const int n = (int)b->members.size();
+    if (n == 0) return LBM_OK;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    DeviceGuard dg(b->device);
+    cudaStream_t st = (cudaStream_t)stream;
+    if (n > b->obs_cap) {
+        const int cap = std::max(n, std::max(16, 2 * b->obs_cap));
+        lbm_observables *d = nullptr;
+        CUDA_TRY(cudaMalloc(&d, (size_t)cap * sizeof(lbm_observables)));
+        if (b->d_obs) {   // earlier calls may still write the old array
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                cudaFree(d);
+                return fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+            }
+            cudaFree(b->d_obs);
+        }
+        b->d_obs = d;
+        b->obs_cap = cap;
+    }
+    for (int i = 0; i < n; i++) {
+        const lbm_case *c = b->members[(size_t)i];
+        if (!c->initialised) return fail(LBM_ERR_STATE, "a member has no state");
+        const int rc = enqueue_observables(c, b->d_obs + i, st);
+        if (rc) return rc;
+    }
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaMemcpyAsync(out, b->d_obs, (size_t)n * sizeof(lbm_observables), cudaMemcpyDefault, st));
     return LBM_OK;
 }
 

@@ -376,9 +376,27 @@ void derive(const lbm_params *p, lbm_derived *d) {
 
 namespace {
 
-int obs_blocks_for(int64_t nodes) {
-    int64_t b = (nodes + kObsThreads - 1) / kObsThreads;
-    return (int)std::max<int64_t>(1, std::min<int64_t>(b, 148 * 8));
+// Most blocks of the observables reduction: 8 per SM of a 148-SM B200.  The
+// fixed array of lbm_observables_noalloc has this many rows, so it covers
+// every grid on every device.
+constexpr int kObsMaxBlocks = 148 * 8;
+
+// SM count of `device` (148 if it cannot be read, e.g. without a GPU)
+int sm_count_of(int device) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess || sms <= 0) {
+        cudaGetLastError();
+        return 148;
+    }
+    return sms;
+}
+
+// Reduction blocks for a grid: one per 256 nodes, at most 8 per SM of the
+// device and never more than kObsMaxBlocks.
+int obs_blocks_for(int64_t nodes, int sms) {
+    const int64_t b = (nodes + kObsThreads - 1) / kObsThreads;
+    const int64_t cap = std::min<int64_t>((int64_t)sms * 8, kObsMaxBlocks);
+    return (int)std::max<int64_t>(1, std::min<int64_t>(b, cap));
 }
 
 template <class S> StepArgs<S> make_args(const lbm_case *c) {
@@ -569,7 +587,8 @@ int lbm_case_bytes(const lbm_params *p, uint64_t *bytes) {
     const int64_t ps = round_up(nodes, 128);
     const uint64_t pop = 2ull * Q * (uint64_t)ps * store_bytes(p->storage);
     const uint64_t carry = (uint64_t)round_up(nodes, 128) * (p->storage == LBM_STORE_F64 ? 8 : 4);
-    const uint64_t scratch = (uint64_t)obs_blocks_for(nodes) * kObs * 8 + 256;
+    // the reduction rows at their most (the device's SM count is not needed)
+    const uint64_t scratch = (uint64_t)obs_blocks_for(nodes, 1 << 20) * kObs * 8 + 256;
     *bytes = pop + carry + scratch;
     return LBM_OK;
 }
@@ -585,8 +604,8 @@ int lbm_create(const lbm_params *p, lbm_case **out) {
     derive(p, &c->d);
     c->nodes = (int64_t)p->lx * p->ly * p->lz;
     c->ps = round_up(c->nodes, 128);
-    c->obs_blocks = obs_blocks_for(c->nodes);
     DeviceGuard dg(p->device);
+    c->obs_blocks = obs_blocks_for(c->nodes, sm_count_of(p->device));
     const size_t sb = store_bytes(p->storage);
     const size_t pop_bytes = (size_t)Q * (size_t)c->ps * sb;
     const size_t carry_bytes = (size_t)c->ps * (p->storage == LBM_STORE_F64 ? 8 : 4);
@@ -805,13 +824,12 @@ int lbm_step(lbm_case *c, int32_t nsteps, void *stream) {
     return LBM_OK;
 }
 
-int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
-    int rc = check_case(c, true);
-    if (rc) return rc;
-    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
-    DeviceGuard dg(c->p.device);
-    cudaStream_t st = (cudaStream_t)stream;
-    rc = with_storage(c, [&](auto tag) {
+}  // extern "C"
+
+// Enqueues on `st` the observables reduction of case c's current state into
+// dst (device memory): two kernels, no synchronisation.
+int lbm_internal::enqueue_observables(const lbm_case *c, lbm_observables *dst, cudaStream_t st) {
+    return with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const StepArgs<S> a = make_args<S>(c);
         LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
@@ -823,9 +841,20 @@ int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
         k.dT = c->p.t_hot - c->p.t_cold;
         k.visc = c->d.visc;
         k.step = c->step;
-        obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, c->d_obs);
+        obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, dst);
         return LBM_OK;
     });
+}
+
+extern "C" {
+
+int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {
+    int rc = check_case(c, true);
+    if (rc) return rc;
+    if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+    DeviceGuard dg(c->p.device);
+    cudaStream_t st = (cudaStream_t)stream;
+    rc = enqueue_observables(c, c->d_obs, st);
     if (rc) return rc;
     CUDA_TRY(cudaGetLastError());
     CUDA_TRY(cudaMemcpyAsync(out, c->d_obs, sizeof(lbm_observables), cudaMemcpyDeviceToHost, st));
@@ -1037,16 +1066,19 @@ int lbm_restore_state(lbm_case *c, const void *host, uint64_t bytes, void *strea
 // array is part of the library image, so every GPU that loads the library
 // holds it (kNoAllocRows x 13 doubles = 123 KB) until the process exits.
 // ---------------------------------------------------------------------------
-constexpr int kNoAllocRows = 148 * 8;   // most reduction blocks one call runs
+constexpr int kNoAllocRows = kObsMaxBlocks;   // most reduction blocks one call runs
+static_assert(kNoAllocRows >= kObsMaxBlocks, "the fixed array must hold every reduction row");
 static __device__ __align__(256) double g_noalloc_partials[kNoAllocRows * kObs];
 
 namespace {
 std::mutex g_noalloc_mu;
 void *g_noalloc_ptr[256];               // device address of the array, per device ordinal
+int g_noalloc_sms[256];                 // SM count, per device ordinal
 
-// Looks up the array's device address once per device, with that device
-// current; host code cannot use the symbol itself as a device address.
-int noalloc_scratch(int device, double **out) {
+// Looks up the array's device address (and the SM count) once per device,
+// with that device current; host code cannot use the symbol itself as a
+// device address.
+int noalloc_scratch(int device, double **out, int *sms) {
     if (device < 0 || device >= 256) return fail(LBM_ERR_ARG, "device ordinal out of range");
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_ptr[device]) {
@@ -1055,9 +1087,11 @@ int noalloc_scratch(int device, double **out) {
         if (e != cudaSuccess || !ptr)
             return fail(LBM_ERR_CUDA, std::string("cudaGetSymbolAddress(g_noalloc_partials): ") +
                                           cudaGetErrorString(e));
+        g_noalloc_sms[device] = sm_count_of(device);
         g_noalloc_ptr[device] = ptr;
     }
     *out = (double *)g_noalloc_ptr[device];
+    *sms = g_noalloc_sms[device];
     return LBM_OK;
 }
 }  // namespace
@@ -1070,14 +1104,22 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
     if (!f || !g || !phi_prev || !out_dev) return fail(LBM_ERR_ARG, "f, g, phi_prev and out_dev are required");
     const int64_t nodes = (int64_t)p->lx * p->ly * p->lz;
     if ((int64_t)pop_stride < nodes) return fail(LBM_ERR_ARG, "pop_stride is smaller than the node count");
-    if (pop_stride > (1ull << 40)) return fail(LBM_ERR_ARG, "pop_stride too large");
-    const int blocks = obs_blocks_for(nodes);
-    if (blocks > kNoAllocRows)
-        return fail(LBM_ERR_ARG, "reduction needs more partial rows than the fixed scratch holds");
+    if (p->storage == LBM_STORE_F16S || p->storage == LBM_STORE_BF16S) {
+        // one array of (f, g) pairs: g is f's partner element, and the pair
+        // rows are addressed with 32-bit indices below 9 * pop_stride
+        if ((const char *)g != (const char *)f + store_bytes(p->storage))
+            return fail(LBM_ERR_ARG, "16-bit storage interleaves f and g: pass g = f + 1 element");
+        if (9ull * pop_stride >= (1ull << 32))
+            return fail(LBM_ERR_ARG, "16-bit storage: pop_stride must be below 477,218,589 pairs");
+    } else if (pop_stride > (1ull << 40)) {
+        return fail(LBM_ERR_ARG, "pop_stride too large");
+    }
     DeviceGuard dg(p->device);
     double *scratch = nullptr;
-    rc = noalloc_scratch(p->device, &scratch);
+    int sms = 0;
+    rc = noalloc_scratch(p->device, &scratch, &sms);
     if (rc) return rc;
+    const int blocks = obs_blocks_for(nodes, sms);   // <= kObsMaxBlocks = the array's rows
     lbm_case view;               // a stack view of the caller's buffers; owns nothing
     view.p = *p;
     derive(p, &view.d);

@@ -47,6 +47,9 @@ void derive(const lbm_params *p, lbm_derived *d);
 int check_params(const lbm_params *p);
 // drops a case that is being destroyed from its batch (batch.cu)
 void batch_forget(lbm_batch *b, lbm_case *c);
+// enqueues the observables reduction of c's current state into dst (device
+// memory) on st, without synchronising (engine.cu)
+int enqueue_observables(const lbm_case *c, lbm_observables *dst, cudaStream_t st);
 
 struct DeviceGuard {
     int prev = -1;

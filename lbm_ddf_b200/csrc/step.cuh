@@ -896,14 +896,16 @@ __device__ __forceinline__ void scatter_half(const A &a, const Node &g, const fl
     });
 }
 
-// Waits until both warps of warp pair `pair` (0 or 1; 64 threads) arrive,
-// on named barrier 1 + pair (immediate ids, so the block reserves three
-// barriers); the non-aligned form, so lanes need not be converged.
+// Waits until both warps of warp pair `pair` (0 to 3; 64 threads) arrive,
+// on named barrier 1 + pair (immediate ids, so the block reserves at most
+// five barriers); the non-aligned form, so lanes need not be converged.
 __device__ __forceinline__ void pair_barrier(int pair) {
-    if (pair == 0)
-        asm volatile("barrier.sync 1, 64;\n" ::: "memory");
-    else
-        asm volatile("barrier.sync 2, 64;\n" ::: "memory");
+    switch (pair) {
+    case 0: asm volatile("barrier.sync 1, 64;\n" ::: "memory"); break;
+    case 1: asm volatile("barrier.sync 2, 64;\n" ::: "memory"); break;
+    case 2: asm volatile("barrier.sync 3, 64;\n" ::: "memory"); break;
+    default: asm volatile("barrier.sync 4, 64;\n" ::: "memory"); break;
+    }
 }
 
 // Half H of the update of node n (valid: n is a node); xch is the warp

@@ -75,8 +75,10 @@ def run_batched(specs, storage="f16s", steps=5000, obs_every=100, tune_steps=2, 
             b.step(nxt - done, stream=stream)
             done = nxt
             if done % obs_every == 0 or done == steps:
-                for i, c in enumerate(cases):
-                    series[i].append(_obs_on(c, stream))
+                # every member's observables in one asynchronous call
+                for i, o in enumerate(b.observables(stream=stream)):
+                    series[i].append({k: o[k] for k in ("step", "nu_bulk", "nu_top", "nu_bottom", "ke", "re",
+                                                        "diverged")})
         stream.synchronize()
         seconds = time.perf_counter() - t0
     nodes = sum(c.n for c in cases)

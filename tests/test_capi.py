@@ -136,3 +136,33 @@ def test_no_gpu_create_fails_cleanly(lbm):
     rc = lbm.lib().lbm_create(C.byref(lbm.make_params(8, 8, 8)), C.byref(h))
     assert rc in (lbm.ERR_CUDA, lbm.ERR_NOMEM)
     assert not h.value
+
+
+def test_noalloc_argument_checks_need_no_gpu(lbm):
+    """lbm_observables_noalloc rejects, before touching a device, a 16-bit
+    call whose g is not f's partner element or whose stride would overflow
+    the 32-bit pair index (9 * pop_stride >= 2^32), and an FP32 stride above
+    2^40; the rejections name the rule."""
+    L = lbm.lib()
+    out = C.c_void_p(4096)
+    pp = C.c_void_p(8192)
+    for st in ("f16s", "bf16s"):
+        p = lbm.make_params(8, 8, 8, storage=st)
+        f = 1 << 20
+        # g elsewhere than f + 1 element
+        rc = L.lbm_observables_noalloc(C.byref(p), C.c_void_p(f), C.c_void_p(f + 4096), pp, 512, 0, 0, out, None)
+        assert rc == lbm.ERR_ARG and "f + 1 element" in L.lbm_last_error().decode()
+        # 477,218,589 is the smallest stride whose nine pair rows overflow
+        # 32-bit indices
+        big = 477_218_589
+        assert 9 * (big - 1) < 2 ** 32 <= 9 * big
+        rc = L.lbm_observables_noalloc(C.byref(p), C.c_void_p(f), C.c_void_p(f + 2), pp, big, 0, 0, out, None)
+        assert rc == lbm.ERR_ARG and "pop_stride" in L.lbm_last_error().decode()
+        rc = L.lbm_observables_noalloc(C.byref(p), C.c_void_p(f), C.c_void_p(f + 2), pp, 2 ** 33, 0, 0, out, None)
+        assert rc == lbm.ERR_ARG
+    p = lbm.make_params(8, 8, 8, storage="f32")
+    rc = L.lbm_observables_noalloc(C.byref(p), C.c_void_p(1 << 20), C.c_void_p(1 << 21), pp, 2 ** 40 + 1, 0, 0,
+                                   out, None)
+    assert rc == lbm.ERR_ARG and "pop_stride" in L.lbm_last_error().decode()
+    rc = L.lbm_observables_noalloc(C.byref(p), C.c_void_p(1 << 20), C.c_void_p(1 << 21), pp, 100, 0, 0, out, None)
+    assert rc == lbm.ERR_ARG   # below the node count

@@ -255,3 +255,31 @@ def test_batch_rejections(lbm):
             b.remove(r)
         with pytest.raises(lbm.LbmError):
             b.set_config(96, 0)
+
+
+@pytest.mark.parametrize("storage", ["f64", "f16s"])
+def test_batch_observables_equal_per_case(lbm, storage):
+    """lbm_batch_observables (one asynchronous call for every member) gives
+    bitwise what lbm_get_observables gives for each member, in member order,
+    also after a removal."""
+    import torch
+
+    cases = make_cases(lbm, storage)
+    with lbm.Batch(storage) as b:
+        for c in cases:
+            b.add(c)
+        b.step(3)
+        got = b.observables()
+        assert [g["step"] for g in got] == [3] * len(cases)
+        for c, g in zip(cases, got):
+            assert g == c.observables()
+        b.remove(cases[1])
+        b.step(2)
+        s = torch.cuda.Stream()
+        s.wait_stream(torch.cuda.current_stream())
+        got = b.observables(stream=s)
+        rest = [c for i, c in enumerate(cases) if i != 1]
+        for c, g in zip(rest, got):
+            assert g == c.observables()
+    for c in cases:
+        c.close()

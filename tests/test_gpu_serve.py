@@ -77,3 +77,31 @@ def test_request_mix_shapes(lbm):
         assert 1.0 <= r.lx / r.ly <= 2.2
         assert 200 <= r.steps <= 5000 and r.steps % 100 == 0
         assert 1e5 <= r.rayleigh <= 1e8 and r.prandtl in (0.71, 4.38) and r.storage in ("f16s", "f32")
+
+
+def test_cancellation_frees_hbm_and_leaves_the_rest_unchanged(lbm):
+    """A running request and one not yet arrived are cancelled: the running
+    one stops part-way with the series it had, every case's HBM is returned,
+    and the other requests' Nu series are bitwise those of a run without the
+    cancellations."""
+    import torch
+
+    from lbm_ddf_b200.serve import Request, Server
+
+    reqs = small_requests(lbm)[:4]
+    reqs[1] = Request(**{**reqs[1].__dict__, "steps": 5000})   # still running when cancelled
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    base = Server(budget_bytes=1e12, obs_every=100).run(reqs, clock=TickClock())
+    srv = Server(budget_bytes=1e12, obs_every=100)
+    res = srv.run(reqs, clock=TickClock(), cancellations=[(0.05, 3), (0.2, 1)])
+    torch.cuda.synchronize()
+    assert res[3].status == "cancelled" and res[3].series == []
+    assert res[1].status == "cancelled" and 0 < res[1].steps < 5000
+    assert res[1].series == base[1].series[:len(res[1].series)]
+    for k in (0, 2):
+        assert res[k].status == "done"
+        assert res[k].series == base[k].series, k
+    assert srv.used == 0
+    free1 = torch.cuda.mem_get_info()[0]
+    assert abs(free1 - free0) <= 64 << 20, (free0, free1)
