@@ -261,6 +261,17 @@ int lbm_step_observed_async(lbm_case *c, int32_t nsteps, lbm_observables *out, v
 int lbm_set_step_kernel(lbm_case *c, int32_t kind);
 int lbm_get_step_kernel(const lbm_case *c, int32_t *kind);
 
+/* Test hook of the row-staged kernel's bounded wait: its steps announce
+ * `bytes` (a multiple of 16, at most 4096; 0 turns the hook off) more on
+ * their shared-memory barrier than their bulk copies bring, so the copies
+ * all land but the wait gives up, after one second, as it would if a copy
+ * never arrived.  The kernel then sets the case's error flag and leaves
+ * the step undone; the next lbm_get_observables returns LBM_ERR_CUDA ("a
+ * step kernel gave up waiting ...") and the CUDA context stays usable.
+ * The state after such a step is unspecified.  No counterpart in the
+ * reference, which has no bounded waits. */
+int lbm_debug_row_wait_extra_bytes(lbm_case *c, uint32_t bytes);
+
 /* Chooses the collision model of a case (LBM_COLLISION_*; BGK at creation),
  * in effect from its next step.  The regularised model runs on the node
  * kernel (and in batches); LBM_ERR_ARG if the case's step kernel is set to

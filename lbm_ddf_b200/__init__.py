@@ -108,6 +108,7 @@ def lib() -> C.CDLL:
         L.lbm_set_step_kernel.argtypes = [vp, C.c_int32]
         L.lbm_get_step_kernel.argtypes = [vp, C.POINTER(C.c_int32)]
         L.lbm_set_collision.argtypes = [vp, C.c_int32]
+        L.lbm_debug_row_wait_extra_bytes.argtypes = [vp, C.c_uint32]
         L.lbm_get_collision.argtypes = [vp, C.POINTER(C.c_int32)]
         L.lbm_batch_create.argtypes = [C.c_int, C.c_int32, C.POINTER(vp)]
         L.lbm_batch_destroy.argtypes = [vp]
@@ -130,7 +131,7 @@ def lib() -> C.CDLL:
                      "lbm_set_collision", "lbm_get_collision", "lbm_step_observed", "lbm_step_observed_async",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
-                     "lbm_batch_autotune", "lbm_batch_observables"):
+                     "lbm_batch_autotune", "lbm_batch_observables", "lbm_debug_row_wait_extra_bytes"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib

@@ -46,10 +46,22 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return done != 0;
 }
 
-// Bounded wait: false if the phase did not complete within max_polls polls.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls) {
-    for (uint32_t i = 0; i < max_polls; i++)
+// nanoseconds of the GPU's global timer
+__device__ __forceinline__ uint64_t global_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: false if the phase did not complete within max_polls polls
+// or max_ns nanoseconds (a poll may suspend the thread for a hardware-
+// dependent time, so the poll count alone does not bound the time).
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t max_polls, uint64_t max_ns) {
+    const uint64_t t0 = global_ns();
+    for (uint32_t i = 0; i < max_polls; i++) {
         if (mbar_try_wait(bar, parity)) return true;
+        if ((i & 63u) == 63u && global_ns() - t0 > max_ns) return false;
+    }
     return false;
 }
 

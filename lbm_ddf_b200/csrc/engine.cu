@@ -507,7 +507,8 @@ cudaError_t launch_row_p(const lbm_case *c, const StepArgs<S> &a, cudaStream_t s
         if (e != cudaSuccess) return e;
         configured.fetch_or(bit, std::memory_order_release);
     }
-    row_step_kernel<S, SW, PITCH><<<(unsigned)(c->p.ly * c->p.lz), (unsigned)c->p.lx, smem, st>>>(a, c->d_err);
+    row_step_kernel<S, SW, PITCH><<<(unsigned)(c->p.ly * c->p.lz), (unsigned)c->p.lx, smem, st>>>(a, c->d_err,
+                                                                                             c->debug_extra_tx);
     return cudaPeekAtLastError();
 }
 
@@ -1182,6 +1183,13 @@ int lbm_set_step_kernel(lbm_case *c, int32_t kind) {
     if (kind == LBM_KERNEL_ROW && c->collision != LBM_COLLISION_BGK)
         return fail(LBM_ERR_ARG, "the row-staged kernel collides with BGK only");
     c->kernel = kind;
+    return LBM_OK;
+}
+
+int lbm_debug_row_wait_extra_bytes(lbm_case *c, uint32_t bytes) {
+    if (!c) return fail(LBM_ERR_ARG, "case is NULL");
+    if (bytes % 16 != 0 || bytes > 4096) return fail(LBM_ERR_ARG, "bytes must be a multiple of 16, at most 4096");
+    c->debug_extra_tx = bytes;
     return LBM_OK;
 }
 

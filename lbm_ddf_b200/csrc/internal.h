@@ -24,6 +24,7 @@ struct lbm_case {
     int32_t collision = LBM_COLLISION_BGK;
     lbm_batch *batch = nullptr;          // the batch the case is a member of
     int *d_err = nullptr;                // set by a step kernel whose bulk-copy wait timed out
+    uint32_t debug_extra_tx = 0;         // lbm_debug_row_wait_extra_bytes (0: off)
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
     int obs_blocks = 0;

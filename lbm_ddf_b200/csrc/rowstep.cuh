@@ -31,7 +31,8 @@
 
 namespace lbm {
 
-constexpr uint32_t kRowMaxPolls = 1u << 22;   // bound on each shared-memory barrier wait
+constexpr uint32_t kRowMaxPolls = 1u << 22;          // bounds on each shared-memory barrier wait:
+constexpr uint64_t kRowMaxNs = 1000000000ull;         // polls and 1 s of the global timer
 
 template <class S> struct RowOccupancy { static constexpr int value = sizeof(S) == 8 ? 1 : 2; };
 
@@ -43,7 +44,12 @@ template <class S> __host__ __device__ constexpr size_t row_smem_bytes(int pitch
 }
 
 template <class S, bool SWAPPED, int PITCH>
-__global__ void __launch_bounds__(256, RowOccupancy<S>::value) row_step_kernel(const StepArgs<S> a, int *err) {
+// extra_tx: bytes announced on the barrier beyond those the copies bring,
+// 0 except in the test of the bounded wait (lbm_debug_row_wait_extra_bytes):
+// the copies then all land but the phase never completes, and the wait runs
+// out as it would if a copy never arrived.
+__global__ void __launch_bounds__(256, RowOccupancy<S>::value) row_step_kernel(const StepArgs<S> a, int *err,
+                                                                             uint32_t extra_tx) {
     using C = Codec<S>;
     using R = typename C::R;
     extern __shared__ __align__(128) unsigned char smem_raw[];
@@ -69,7 +75,7 @@ __global__ void __launch_bounds__(256, RowOccupancy<S>::value) row_step_kernel(c
     }
     __syncthreads();
     if (x == 0) {
-        bulk::mbar_expect_tx(bar, 2u * Q * bytes);
+        bulk::mbar_expect_tx(bar, 2u * Q * bytes + extra_tx);
         Unroll<0, Q>::run([&](auto kk) {
             constexpr int K = decltype(kk)::value;
             const S *fsrc;
@@ -94,8 +100,13 @@ __global__ void __launch_bounds__(256, RowOccupancy<S>::value) row_step_kernel(c
     }
     const uint32_t n = row * (uint32_t)lx + (uint32_t)x;
     const R pp = (R)a.phip[n];
-    const bool ok = bulk::mbar_wait(bar, 0, kRowMaxPolls);
-    if (!ok) atomicOr(err, 1);
+    const bool ok = bulk::mbar_wait(bar, 0, kRowMaxPolls, kRowMaxNs);
+    if (!ok) {
+        atomicOr(err, 1);
+        // copies still on their way land in this block's shared memory: give
+        // them one more bounded wait before the block leaves it
+        (void)bulk::mbar_wait(bar, 0, kRowMaxPolls, kRowMaxNs);
+    }
     if (!__syncthreads_and(ok)) return;   // the whole block leaves together
 
     const int xm = x == 0 ? lx - 1 : x - 1;
