@@ -5,9 +5,7 @@
 // AA layout and collision model; one launch of batch_step_kernel per
 // non-empty group (normally one: members move through the layouts in step)
 // advances the group's members by one step.  Their nodes are cut into tiles
-// of kTileRounds x BLOCK nodes (x BLOCK / 2 for 16-bit BGK members, whose
-// node updates are split over two warps, batch_step16_split_kernel),
-// numbered case after case; blocks walk the tile list with a
+// of kTileRounds x BLOCK nodes, numbered case after case; blocks walk the tile list with a
 // grid stride (persistent blocks, BLOCKS_PER_SM x 148 of them, or one block
 // per tile), find each tile's case by a binary search over the tiles' prefix
 // sums held in shared memory, and apply the same node update as the
@@ -118,55 +116,6 @@ __global__ void __launch_bounds__(BLOCK, BatchOccupancy<S, BLOCK>::value)
     }
 }
 
-// 16-bit storage, BGK: the members' node updates split over two warps, as in
-// the single-case step16_split_kernel (step.cuh split_update): warps 2p and
-// 2p + 1 of a block share 32 nodes, each loading, relaxing and storing half
-// of the populations.  A tile is kTileRounds rounds of BLOCK / 2 nodes of one
-// member.  A warp pair exchanges its partial moments once per round through
-// a two-buffer area (the partner reads round r's buffer before it reaches
-// the barrier of round r + 1, which the writer of round r + 2 has passed).
-// The tile prefix sums are in dynamic shared memory ((ncases + 1) words), so
-// kSplitBlocks blocks of 128 threads fit on an SM.
-template <int BLOCK> struct SplitBatchOccupancy {
-    static constexpr int value = kSplitBlocks * 128 / BLOCK;
-};
-
-template <class S, int BLOCK, bool SWAPPED>
-__global__ void __launch_bounds__(BLOCK, SplitBatchOccupancy<BLOCK>::value)
-    batch_step16_split_kernel(const BatchCase<S> *__restrict__ cases, int ncases,
-                              const uint32_t *__restrict__ tile_start) {
-    static_assert(BLOCK == 128 || BLOCK == 256, "two or four warp pairs");
-    extern __shared__ uint32_t s_start[];
-    __shared__ float xch[BLOCK / 64][2][2][5][32];   // [warp pair][buffer][half][moment][lane]
-    for (int i = threadIdx.x; i <= ncases; i += BLOCK) s_start[i] = tile_start[i];
-    __syncthreads();
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int pair = warp >> 1;
-    constexpr uint32_t kRound = BLOCK / 2;            // nodes per round
-    const uint32_t end = s_start[ncases];
-    int buf = 0;
-    for (uint32_t t = s_start[0] + blockIdx.x; t < end; t += gridDim.x) {
-        int lo = 0, hi = ncases;   // the member c with s_start[c] <= t < s_start[c+1]
-        while (hi - lo > 1) {
-            const int mid = (lo + hi) >> 1;
-            if (s_start[mid] <= t) lo = mid;
-            else hi = mid;
-        }
-        const BatchCase<S> &cs = cases[lo];
-        const uint32_t u0 = (t - s_start[lo]) * (kRound * kTileRounds) + (uint32_t)(pair * 32 + lane);
-#pragma unroll 1
-        for (int r = 0; r < kTileRounds; r++) {
-            const uint32_t u = u0 + r * kRound;
-            const bool valid = u < cs.nodes;
-            if ((warp & 1) == 0)
-                split_update<0, S, SWAPPED, true>(cs, u, valid, xch[pair][buf], lane, pair);
-            else
-                split_update<1, S, SWAPPED, true>(cs, u, valid, xch[pair][buf], lane, pair);
-            buf ^= 1;
-        }
-    }
-}
-
 }  // namespace lbm
 
 struct lbm_batch {
@@ -270,13 +219,6 @@ int group_of(const lbm_batch *b, const lbm_case *c) {
     return ((c->swapped ? 1 : 0) ^ b->phase) | (c->collision == LBM_COLLISION_REGULARIZED ? 2 : 0);
 }
 
-// Nodes per tile of a member: kTileRounds rounds of the block's threads, or
-// of half of them where two warps share each node (16-bit BGK members).
-int64_t tile_nodes(const lbm_batch *b, const lbm_case *c) {
-    const bool split = interleaved(c) && c->collision == LBM_COLLISION_BGK;
-    return (int64_t)(split ? b->block / 2 : b->block) * kTileRounds;
-}
-
 // Rebuilds and uploads the descriptors after a membership change.
 int refresh(lbm_batch *b, cudaStream_t st) {
     if (!b->dirty) return LBM_OK;
@@ -317,7 +259,7 @@ int refresh(lbm_batch *b, cudaStream_t st) {
             const BatchCase<S> d = describe<S>(order[(size_t)i]);
             std::memcpy(b->h_cases.data() + (size_t)i * db, &d, db);
             b->h_start[i] = tiles;
-            const int64_t tile = tile_nodes(b, order[(size_t)i]);
+            const int64_t tile = (int64_t)b->block * kTileRounds;
             tiles += (uint32_t)((order[(size_t)i]->nodes + tile - 1) / tile);
         }
         return LBM_OK;
@@ -359,14 +301,8 @@ unsigned grid_of(const lbm_batch *b, uint32_t tiles) {
 
 template <class S, int BLOCK, bool SW>
 void launch_group(const BatchCase<S> *cases, int n, const uint32_t *start, bool reg, unsigned grid, cudaStream_t st) {
-    if (reg) {
-        batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_REGULARIZED><<<grid, BLOCK, 0, st>>>(cases, n, start);
-    } else if constexpr (sizeof(S) == 2) {   // 16-bit BGK: two warps per node
-        batch_step16_split_kernel<S, BLOCK, SW><<<grid, BLOCK, (size_t)(n + 1) * sizeof(uint32_t), st>>>(cases, n,
-                                                                                                        start);
-    } else {
-        batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
-    }
+    if (reg) batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_REGULARIZED><<<grid, BLOCK, 0, st>>>(cases, n, start);
+    else batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
 }
 
 // Enqueues `nsteps` batch steps on `st`: per step one launch per non-empty

@@ -79,10 +79,10 @@ __global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, d
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < a.nodes; n += gridDim.x * blockDim.x) {
         const Node g = make_node<PERIODIC>(a, n);
         R fr[Q], gr[Q];
-        // rows away from the plates of a periodic box: no boundary tests
-        // (uniform over a warp whenever LX is a multiple of 32); FP64 keeps
-        // one path (two do not fit its registers)
-        if (sizeof(S) < 8 && SWAPPED && PERIODIC && g.vym && g.vyp)
+        // rows away from the plates (and a closed box's z walls): no y or z
+        // boundary tests (uniform over a warp whenever LX is a multiple of
+        // 32); FP64 keeps one path (two do not fit its registers)
+        if (sizeof(S) < 8 && SWAPPED && yz_interior<PERIODIC>(g))
             gather<S, SWAPPED, true>(a, g, fr, gr);
         else
             gather<S, SWAPPED, false>(a, g, fr, gr);

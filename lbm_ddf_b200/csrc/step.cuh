@@ -167,11 +167,22 @@ __device__ __forceinline__ bool inside(const Node &g) {
     return (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) && (DY < 0 ? g.vym : DY > 0 ? g.vyp : true) &&
            (DZ < 0 ? g.vzm : DZ > 0 ? g.vzp : true);
 }
-// With INTERIOR set the caller guarantees every neighbour is inside the box
-// (periodic sides and 0 < iy < LY-1), so no test is made.
+// With INTERIOR set the caller guarantees that the neighbours along y and z
+// are inside the box (0 < iy < LY-1, and periodic sides or 0 < iz < LZ-1),
+// so only the x neighbour is tested (a compile-time true with periodic
+// sides; a per-lane select at the x walls of a closed box, where the node's
+// warp still takes this path, since a warp lies in one row when LX is a
+// multiple of 32).
 template <bool INTERIOR, int DX, int DY, int DZ>
 __device__ __forceinline__ bool inside_t(const Node &g) {
-    return INTERIOR ? true : inside<DX, DY, DZ>(g);
+    return INTERIOR ? (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) : inside<DX, DY, DZ>(g);
+}
+
+// Whether node g's neighbours along y and z are all inside the box (the
+// INTERIOR case of inside_t); uniform over a warp whenever LX is a multiple
+// of 32.
+template <bool PERIODIC> __device__ __forceinline__ bool yz_interior(const Node &g) {
+    return g.vym && g.vyp && (PERIODIC || (g.vzm && g.vzp));
 }
 
 // Population k (of f when WHICH = 0, of g when 1) of node g at the current
@@ -497,7 +508,7 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
         R fv = fr[I];
         R gv = gr[I];
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-        const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
         if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: f/w and g/w - T_c at the location, packed
             // the location's T_c is s0 - write_shift_delta (it is s0 at the node itself)
@@ -623,18 +634,20 @@ template <class R> struct NodeOut {
 // Opposite directions share c.u and the quadratic part of p.  The same
 // update as collide_fast, with fewer instructions per node.
 
-template <class S, bool SWAPPED, bool INTERIOR, class A>
+template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
 __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
         fh[K] = v.x;
         gh[K] = v.y;
-        // relative to the node's T_c; on interior rows of the swapped layout
-        // the read and write re-referencing is folded into the collision
-        // (collide_norm's `fold`), as the moments do not see it (the deltas
-        // of each weight class sum to zero)
-        if constexpr (!(INTERIOR && SWAPPED)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+        // relative to the node's T_c; on interior rows of a periodic box in
+        // the swapped layout the read and write re-referencing is folded
+        // into the collision (collide_norm's `fold`), as the moments do not
+        // see it (the deltas of each weight class sum to zero); a closed
+        // box's x walls keep some populations in the node's own plane, so
+        // there each delta is applied
+        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
     });
 }
 
@@ -675,8 +688,8 @@ __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], con
 // opposite directions: two multiply-adds per population and three per pair.
 // (gh = g/w - s0; t0 enters only the buoyancy force.)  fold: the plane
 // spacing of the conduction profile when gh holds raw stored values that
-// were read from, and go to, the planes y - c_y and y + c_y (interior rows,
-// swapped layout): ag (v + c_y fold) + ... + c_y fold = ag v + ... +
+// were read from, and go to, the planes y - c_y and y + c_y (interior rows
+// of a periodic box, swapped layout): ag (v + c_y fold) + ... + c_y fold = ag v + ... +
 // (ag + 1) c_y fold, one more coefficient per c_y; else 0.
 __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
                                              float om_g, float force_fac, float gbeta, float t0, float s0,
@@ -725,11 +738,11 @@ __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const fl
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
         float gv = gh[I];
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-        const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
         // relative to T_c at the location written (folded into the
-        // collision on interior rows of the swapped layout)
-        if constexpr (!(INTERIOR && SWAPPED)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
+        // collision on interior rows of a periodic box's swapped layout)
+        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
         const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
             a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -742,16 +755,16 @@ template <class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t n) {
     const Node g = make_node<PERIODIC>(a, n);
     float fh[Q], gh[Q];
-    const bool interior = PERIODIC && g.vym && g.vyp;
+    const bool interior = yz_interior<PERIODIC>(g);
     if (interior)
-        gather_norm<S, SWAPPED, true>(a, g, fh, gh);
+        gather_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh);
     else
-        gather_norm<S, SWAPPED, false>(a, g, fh, gh);
+        gather_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh);
     const float s0 = shift0(a, g);
     Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0, s0);
     if (a.use_phi_fix) m.phi = a.phi_fix;
     collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
-                 SWAPPED && interior ? (float)a.t_dy : 0.f);
+                 SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
     a.phip[n] = m.phi;
     if (interior)
         scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
@@ -796,7 +809,7 @@ __host__ __device__ constexpr bool split_halves_ok() {
 }
 static_assert(split_halves_ok(), "split update: bad population halves");
 
-template <int H, class S, bool SWAPPED, bool INTERIOR, class A>
+template <int H, class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
 __device__ __forceinline__ void gather_half(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
@@ -804,7 +817,7 @@ __device__ __forceinline__ void gather_half(const A &a, const Node &g, float (&f
             const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
             fh[K] = v.x;
             gh[K] = v.y;
-            if constexpr (!(INTERIOR && SWAPPED)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
         }
     });
 }
@@ -884,9 +897,9 @@ __device__ __forceinline__ void scatter_half(const A &a, const Node &g, const fl
             constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
             float gv = gh[I];
             const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-            const bool out_z = !PERIODIC && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+            const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
             if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
-            if constexpr (!(INTERIOR && SWAPPED)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
+            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
             const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
             if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
                 a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -896,16 +909,14 @@ __device__ __forceinline__ void scatter_half(const A &a, const Node &g, const fl
     });
 }
 
-// Waits until both warps of warp pair `pair` (0 to 3; 64 threads) arrive,
-// on named barrier 1 + pair (immediate ids, so the block reserves at most
-// five barriers); the non-aligned form, so lanes need not be converged.
+// Waits until both warps of warp pair `pair` (0 or 1; 64 threads) arrive,
+// on named barrier 1 + pair (immediate ids, so the block reserves three
+// barriers); the non-aligned form, so lanes need not be converged.
 __device__ __forceinline__ void pair_barrier(int pair) {
-    switch (pair) {
-    case 0: asm volatile("barrier.sync 1, 64;\n" ::: "memory"); break;
-    case 1: asm volatile("barrier.sync 2, 64;\n" ::: "memory"); break;
-    case 2: asm volatile("barrier.sync 3, 64;\n" ::: "memory"); break;
-    default: asm volatile("barrier.sync 4, 64;\n" ::: "memory"); break;
-    }
+    if (pair == 0)
+        asm volatile("barrier.sync 1, 64;\n" ::: "memory");
+    else
+        asm volatile("barrier.sync 2, 64;\n" ::: "memory");
 }
 
 // Half H of the update of node n (valid: n is a node); xch is the warp
@@ -922,11 +933,11 @@ __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid,
     if (valid) {
         phip = a.phip[n];   // before the barrier: half 0 overwrites it after
         g = make_node<PERIODIC>(a, n);
-        interior = PERIODIC && g.vym && g.vyp;
+        interior = yz_interior<PERIODIC>(g);
         if (interior)
-            gather_half<H, S, SWAPPED, true>(a, g, fh, gh);
+            gather_half<H, S, SWAPPED, PERIODIC, true>(a, g, fh, gh);
         else
-            gather_half<H, S, SWAPPED, false>(a, g, fh, gh);
+            gather_half<H, S, SWAPPED, PERIODIC, false>(a, g, fh, gh);
         partial_moments<H>(fh, gh, p);
     }
 #pragma unroll
@@ -945,7 +956,7 @@ __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid,
     m.phi = tot[4] + s0;
     if (a.use_phi_fix) m.phi = a.phi_fix;
     collide_half<H>(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
-                    SWAPPED && interior ? (float)a.t_dy : 0.f);
+                    SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
     if (H == 0) a.phip[n] = m.phi;
     if (interior)
         scatter_half<H, S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
@@ -961,9 +972,10 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     using R = typename Codec<S>::R;
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
-    // Periodic sides: rows away from the plates need no boundary tests.  The
-    // branch is uniform over a warp whenever LX is a multiple of 32.
-    const bool interior = PERIODIC && g.vym && g.vyp;
+    // Rows away from the plates (and, in a closed box, from the z walls)
+    // need no y or z boundary tests; the branch is uniform over a warp
+    // whenever LX is a multiple of 32.
+    const bool interior = yz_interior<PERIODIC>(g);
     if (interior)
         gather<S, SWAPPED, true>(a, g, fr, gr);
     else

@@ -330,6 +330,33 @@ def test_reduced_precision_vs_oracle(lbm, oracle_mod, storage, tol, steps, perio
     assert abs(got["obs"]["nu_bulk"] - ob["nu_bulk"]) <= 50 * tol
 
 
+# Bounds on the signed mean error (field-relative) after 400 steps, about 10x
+# the values measured on B200 (FP16S: phi 1.2e-7, g 1.5e-8; BF16S: phi 2.2e-6,
+# g 2.7e-7).  Round-to-nearest storage leaves errors of both signs, so their
+# mean is ~100x below their maximum; a systematic bias of even 1% of a
+# 16-bit ulp per step would shift the mean past these bounds within 400
+# steps, which the max-error bounds above would not notice.
+BIAS_BOUNDS = {"f16s": {"phi": 2e-6, "g": 4e-7}, "bf16s": {"phi": 2e-5, "g": 4e-6}}
+
+
+@pytest.mark.parametrize("storage", ["f16s", "bf16s"])
+@pytest.mark.parametrize("periodic", [True, False])
+def test_16bit_storage_has_no_systematic_bias(lbm, oracle_mod, storage, periodic):
+    lx, ly, lz, steps = 24, 20, 16, 400
+    o = oracle_run(oracle_mod, lx, ly, lz, steps, periodic, seed=21, amplitude=1e-2, ra=1e6)
+    p = lbm.make_params(lx, ly, lz, rayleigh=1e6, prandtl=0.71, storage=storage,
+                        sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL)
+    with lbm.Case(p) as c:
+        c.init_conduction(21, 1e-2)
+        c.step(steps)
+        got = c.store_ref_state(("phi", "g"))
+    for k, bound in BIAS_BOUNDS[storage].items():
+        ref = o.field(k).reshape(got[k].shape)
+        mean = float(np.mean(got[k] - ref)) / float(np.max(np.abs(ref)))
+        assert abs(mean) <= bound, (storage, periodic, k, mean)
+    o.close()
+
+
 # ---------------------------------------------------------------- regularised collision
 
 @pytest.mark.parametrize("storage,tol,steps", [("f64", 1e-12, 200), ("f32", 5e-5, 200), ("f16s", 5e-3, 100),
