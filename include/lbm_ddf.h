@@ -317,9 +317,23 @@ int lbm_batch_observables(lbm_batch *b, lbm_observables *out, void *stream);
  * graphs for multi-step calls. */
 int lbm_batch_set_config(lbm_batch *b, int32_t block, int32_t blocks_per_sm, int32_t use_graph);
 int lbm_batch_get_config(const lbm_batch *b, int32_t *block, int32_t *blocks_per_sm, int32_t *use_graph);
-/* Times every launch shape on 2 x steps_per_trial real steps of the batch
- * (the shapes compute identical per-node arithmetic, so the steps count),
- * keeps the fastest and reports it; steps_per_trial must be even. */
+/* How a batch step is launched.  LBM_BATCH_TILES (the default): one
+ * persistent kernel per group of members walks every member's tiles (the
+ * launch shape above).  LBM_BATCH_PER_CASE: each member's own single-case
+ * step kernel (the one lbm_step launches, its parameters in the constant
+ * bank), the members spread over 8 streams forked from and joined to the
+ * batch's stream, so in a captured graph they run as parallel branches;
+ * results are bitwise those of lbm_step.  Both give every member the same
+ * state. */
+#define LBM_BATCH_TILES 0
+#define LBM_BATCH_PER_CASE 1
+int lbm_batch_set_launch(lbm_batch *b, int32_t launch);
+int lbm_batch_get_launch(const lbm_batch *b, int32_t *launch);
+/* Times every launch (the tile walk's shapes and the per-case launch) on
+ * 2 x steps_per_trial real steps of the batch (all compute identical
+ * per-node arithmetic for a member, so the steps count), keeps the fastest
+ * and reports it (lbm_batch_get_launch tells which launch won);
+ * steps_per_trial must be even. */
 int lbm_batch_autotune(lbm_batch *b, int32_t steps_per_trial, void *stream, int32_t *block,
                        int32_t *blocks_per_sm, double *best_ms_per_step);
 

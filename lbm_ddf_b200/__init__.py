@@ -32,6 +32,8 @@ STORAGE_NAMES = {"f64": STORE_F64, "f32": STORE_F32, "f16s": STORE_F16S, "bf16s"
 STORAGE_BYTES = {STORE_F64: 8, STORE_F32: 4, STORE_F16S: 2, STORE_BF16S: 2}
 KERNEL_AUTO, KERNEL_NODE, KERNEL_ROW = 0, 1, 2
 COLLISION_BGK, COLLISION_REGULARIZED = 0, 1
+BATCH_TILES, BATCH_PER_CASE = 0, 1
+BATCH_LAUNCH_NAMES = {"tiles": BATCH_TILES, "per_case": BATCH_PER_CASE}
 COLLISION_NAMES = {"bgk": COLLISION_BGK, "regularized": COLLISION_REGULARIZED}
 
 
@@ -117,6 +119,8 @@ def lib() -> C.CDLL:
         L.lbm_batch_size.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_uint64)]
         L.lbm_batch_step.argtypes = [vp, C.c_int32, vp]
         L.lbm_batch_observables.argtypes = [vp, vp, vp]
+        L.lbm_batch_set_launch.argtypes = [vp, C.c_int32]
+        L.lbm_batch_get_launch.argtypes = [vp, C.POINTER(C.c_int32)]
         L.lbm_batch_set_config.argtypes = [vp, C.c_int32, C.c_int32, C.c_int32]
         L.lbm_batch_get_config.argtypes = [vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32), C.POINTER(C.c_int32)]
         L.lbm_batch_autotune.argtypes = [vp, C.c_int32, vp, C.POINTER(C.c_int32), C.POINTER(C.c_int32),
@@ -131,7 +135,8 @@ def lib() -> C.CDLL:
                      "lbm_set_collision", "lbm_get_collision", "lbm_step_observed", "lbm_step_observed_async",
                      "lbm_batch_create", "lbm_batch_destroy", "lbm_batch_add", "lbm_batch_remove",
                      "lbm_batch_size", "lbm_batch_step", "lbm_batch_set_config", "lbm_batch_get_config",
-                     "lbm_batch_autotune", "lbm_batch_observables", "lbm_debug_row_wait_extra_bytes"):
+                     "lbm_batch_autotune", "lbm_batch_observables", "lbm_debug_row_wait_extra_bytes",
+                     "lbm_batch_set_launch", "lbm_batch_get_launch"):
             getattr(L, name).restype = C.c_int
         _lib = L
     return _lib
@@ -516,13 +521,25 @@ class Batch:
     def set_config(self, block: int = 128, blocks_per_sm: int = 0, use_graph: bool = True):
         check(lib().lbm_batch_set_config(self._h, block, blocks_per_sm, int(bool(use_graph))))
 
+    def set_launch(self, launch):
+        """'tiles' (one persistent kernel walks every member's tiles; the
+        default) or 'per_case' (each member's own single-case kernel, the
+        members on parallel streams)."""
+        check(lib().lbm_batch_set_launch(self._h, BATCH_LAUNCH_NAMES.get(launch, launch)))
+
+    @property
+    def launch(self) -> str:
+        m = C.c_int32()
+        check(lib().lbm_batch_get_launch(self._h, C.byref(m)))
+        return next(k for k, v in BATCH_LAUNCH_NAMES.items() if v == m.value)
+
     def config(self) -> dict:
         b, p, g = C.c_int32(), C.c_int32(), C.c_int32()
         check(lib().lbm_batch_get_config(self._h, C.byref(b), C.byref(p), C.byref(g)))
-        return {"block": b.value, "blocks_per_sm": p.value, "use_graph": bool(g.value)}
+        return {"block": b.value, "blocks_per_sm": p.value, "use_graph": bool(g.value), "launch": self.launch}
 
     def autotune(self, steps_per_trial: int = 4, stream=None) -> dict:
         b, p, ms = C.c_int32(), C.c_int32(), C.c_double()
         check(lib().lbm_batch_autotune(self._h, steps_per_trial, _stream_handle(stream), C.byref(b), C.byref(p),
                                        C.byref(ms)))
-        return {"block": b.value, "blocks_per_sm": p.value, "ms_per_step": ms.value}
+        return {"block": b.value, "blocks_per_sm": p.value, "ms_per_step": ms.value, "launch": self.launch}

@@ -36,6 +36,7 @@ using namespace lbm_internal;
 namespace lbm {
 
 constexpr int kMaxBatch = 2048;    // members per batch (tile prefix sums in shared memory)
+constexpr int kLanes = 8;          // streams of the one-kernel-per-member launch
 // A tile is kTileRounds rounds of BLOCK nodes of one member, so the member
 // lookup (binary search, descriptor) is paid once per kTileRounds nodes a
 // thread updates (96-case FP16S ensemble on B200: 19.3, 19.9, 20.5 and 20.6
@@ -153,6 +154,12 @@ struct lbm_batch {
     std::map<int, cudaGraphExec_t> graphs;
     cudaStream_t capture_stream = nullptr;
     int sm_count = 148;
+    // LBM_BATCH_PER_CASE: each member's own single-case kernel, the members
+    // spread round-robin over kLanes streams forked from and joined to the
+    // stepping stream (created on first use)
+    int32_t launch = LBM_BATCH_TILES;
+    cudaStream_t lanes[kLanes] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kLanes] = {};
 };
 
 namespace {
@@ -305,9 +312,40 @@ void launch_group(const BatchCase<S> *cases, int n, const uint32_t *start, bool 
     else batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
 }
 
+// LBM_BATCH_PER_CASE: `nsteps` steps of every member, each through its own
+// single-case node kernel (its parameters in the constant bank, as lbm_step
+// launches it), member i on lane i mod kLanes; the lanes are forked from
+// and joined to `st` by events, so captured into a graph the members' steps
+// are parallel branches and the kernels of different members run
+// concurrently.
+int enqueue_steps_per_case(lbm_batch *b, int nsteps, cudaStream_t st) {
+    if (!b->fork_ev) {
+        CUDA_TRY(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+        for (int l = 0; l < kLanes; l++) {
+            CUDA_TRY(cudaStreamCreateWithFlags(&b->lanes[l], cudaStreamNonBlocking));
+            CUDA_TRY(cudaEventCreateWithFlags(&b->join_ev[l], cudaEventDisableTiming));
+        }
+    }
+    const int nl = std::min<int>(kLanes, (int)b->members.size());
+    CUDA_TRY(cudaEventRecord(b->fork_ev, st));
+    for (int l = 0; l < nl; l++) CUDA_TRY(cudaStreamWaitEvent(b->lanes[l], b->fork_ev, 0));
+    for (int s = 0; s < nsteps; s++)
+        for (size_t i = 0; i < b->members.size(); i++) {
+            const lbm_case *c = b->members[i];
+            const int rc = enqueue_case_step(c, c->swapped != ((s & 1) != 0), b->lanes[i % kLanes]);
+            if (rc) return rc;
+        }
+    for (int l = 0; l < nl; l++) {
+        CUDA_TRY(cudaEventRecord(b->join_ev[l], b->lanes[l]));
+        CUDA_TRY(cudaStreamWaitEvent(st, b->join_ev[l], 0));
+    }
+    return LBM_OK;
+}
+
 // Enqueues `nsteps` batch steps on `st`: per step one launch per non-empty
 // group, in the layout its members are in at that step.
 int enqueue_steps(lbm_batch *b, int nsteps, cudaStream_t st) {
+    if (b->launch == LBM_BATCH_PER_CASE) return enqueue_steps_per_case(b, nsteps, st);
     return with_batch_storage(b, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const BatchCase<S> *cases = (const BatchCase<S> *)b->d_cases;
@@ -385,6 +423,11 @@ int lbm_batch_destroy(lbm_batch *b) {
     cudaFree(b->d_cases);
     cudaFree(b->d_start);
     cudaFree(b->d_obs);
+    for (int l = 0; l < kLanes; l++) {
+        if (b->lanes[l]) cudaStreamDestroy(b->lanes[l]);
+        if (b->join_ev[l]) cudaEventDestroy(b->join_ev[l]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
     for (int i = 0; i < 2; i++) {
         if (b->stage_ev[i]) {
             cudaEventSynchronize(b->stage_ev[i]);
@@ -447,6 +490,20 @@ int lbm_batch_set_config(lbm_batch *b, int32_t block, int32_t blocks_per_sm, int
     b->blocks_per_sm = blocks_per_sm;
     b->use_graph = use_graph != 0;
     drop_graphs(b);
+    return LBM_OK;
+}
+
+int lbm_batch_set_launch(lbm_batch *b, int32_t launch) {
+    if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+    if (launch != LBM_BATCH_TILES && launch != LBM_BATCH_PER_CASE) return fail(LBM_ERR_ARG, "unknown batch launch");
+    if (launch != b->launch) drop_graphs(b);
+    b->launch = launch;
+    return LBM_OK;
+}
+
+int lbm_batch_get_launch(const lbm_batch *b, int32_t *launch) {
+    if (!b || !launch) return fail(LBM_ERR_ARG, "NULL argument");
+    *launch = b->launch;
     return LBM_OK;
 }
 
@@ -535,45 +592,50 @@ int lbm_batch_autotune(lbm_batch *b, int32_t steps_per_trial, void *stream, int3
     if (b->members.empty()) return fail(LBM_ERR_STATE, "batch is empty");
     DeviceGuard dg(b->device);
     cudaStream_t st = (cudaStream_t)stream;
-    const int blocks[2] = {128, 256};
-    const int per_sm[5] = {0, 4, 8, 16, 32};
+    // candidates: the tile walk at 2 block sizes x 5 grids, and one kernel per member
+    struct Shape {
+        int32_t launch, block, per_sm;
+    };
+    std::vector<Shape> shapes;
+    for (int blk : {128, 256})
+        for (int ps : {0, 4, 8, 16, 32}) shapes.push_back({LBM_BATCH_TILES, blk, ps});
+    shapes.push_back({LBM_BATCH_PER_CASE, 128, 0});   // the tile shape is then unused
     cudaEvent_t e0, e1;
     CUDA_TRY(cudaEventCreate(&e0));
     CUDA_TRY(cudaEventCreate(&e1));
     double best = 1e30;
-    int bb = b->block, bp = b->blocks_per_sm;
+    Shape keep{b->launch, b->block, b->blocks_per_sm};
     const bool graph = b->use_graph;
     int rc = LBM_OK;
-    for (int bi = 0; bi < 2 && rc == LBM_OK; bi++)
-        for (int pi = 0; pi < 5 && rc == LBM_OK; pi++) {
-            rc = lbm_batch_set_config(b, blocks[bi], per_sm[pi], graph);
-            if (rc) break;
-            rc = lbm_batch_step(b, steps_per_trial, stream);   // warm-up (and graph capture)
-            if (rc) break;
-            cudaEventRecord(e0, st);
-            rc = lbm_batch_step(b, steps_per_trial, stream);
-            if (rc) break;
-            cudaEventRecord(e1, st);
-            cudaError_t e = cudaEventSynchronize(e1);
-            if (e != cudaSuccess) {
-                rc = fail(LBM_ERR_CUDA, cudaGetErrorString(e));
-                break;
-            }
-            float ms = 0;
-            cudaEventElapsedTime(&ms, e0, e1);
-            if (ms / steps_per_trial < best) {
-                best = ms / steps_per_trial;
-                bb = blocks[bi];
-                bp = per_sm[pi];
-            }
+    for (const Shape &sh : shapes) {
+        rc = lbm_batch_set_config(b, sh.block, sh.per_sm, graph);
+        if (!rc) rc = lbm_batch_set_launch(b, sh.launch);
+        if (!rc) rc = lbm_batch_step(b, steps_per_trial, stream);   // warm-up (and graph capture)
+        if (rc) break;
+        cudaEventRecord(e0, st);
+        rc = lbm_batch_step(b, steps_per_trial, stream);
+        if (rc) break;
+        cudaEventRecord(e1, st);
+        cudaError_t e = cudaEventSynchronize(e1);
+        if (e != cudaSuccess) {
+            rc = fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+            break;
         }
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        if (ms / steps_per_trial < best) {
+            best = ms / steps_per_trial;
+            keep = sh;
+        }
+    }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     if (rc) return rc;
-    rc = lbm_batch_set_config(b, bb, bp, graph);
+    rc = lbm_batch_set_config(b, keep.block, keep.per_sm, graph);
+    if (!rc) rc = lbm_batch_set_launch(b, keep.launch);
     if (rc) return rc;
-    if (block) *block = bb;
-    if (blocks_per_sm) *blocks_per_sm = bp;
+    if (block) *block = keep.block;
+    if (blocks_per_sm) *blocks_per_sm = keep.per_sm;
     if (best_ms_per_step) *best_ms_per_step = best;
     return LBM_OK;
 }

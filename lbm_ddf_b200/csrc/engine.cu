@@ -847,6 +847,27 @@ int lbm_internal::enqueue_observables(const lbm_case *c, lbm_observables *dst, c
     });
 }
 
+// Enqueues on `st` one node-kernel step of case c from layout `swapped`
+// (whatever c->swapped says: a batch enqueues several steps of a member
+// before its host-side layout flag moves); changes nothing on the host.
+int lbm_internal::enqueue_case_step(const lbm_case *c, bool swapped, cudaStream_t st) {
+    return with_storage(c, [&](auto tag) {
+        using S = std::remove_pointer_t<decltype(tag)>;
+        StepArgs<S> a = make_args<S>(c);
+        a.use_phi_fix = 0;   // batch members have taken their first step
+        const bool per = c->p.sides == LBM_SIDES_PERIODIC;
+        if (swapped) {
+            if (per) launch_step_t<S, true, true>(c, a, st);
+            else launch_step_t<S, true, false>(c, a, st);
+        } else {
+            if (per) launch_step_t<S, false, true>(c, a, st);
+            else launch_step_t<S, false, false>(c, a, st);
+        }
+        const cudaError_t e = cudaPeekAtLastError();
+        return e == cudaSuccess ? LBM_OK : fail(LBM_ERR_CUDA, cudaGetErrorString(e));
+    });
+}
+
 extern "C" {
 
 int lbm_get_observables(lbm_case *c, lbm_observables *out, void *stream) {

@@ -51,6 +51,9 @@ void batch_forget(lbm_batch *b, lbm_case *c);
 // enqueues the observables reduction of c's current state into dst (device
 // memory) on st, without synchronising (engine.cu)
 int enqueue_observables(const lbm_case *c, lbm_observables *dst, cudaStream_t st);
+// enqueues one node-kernel step of c from layout `swapped` on st; the host
+// state (step count, layout flag) is the caller's to advance (engine.cu)
+int enqueue_case_step(const lbm_case *c, bool swapped, cudaStream_t st);
 
 struct DeviceGuard {
     int prev = -1;

@@ -136,13 +136,15 @@ def test_persistent_shapes_and_autotune(lbm):
         b.step(2)
         b.set_config(128, 2, use_graph=False)
         b.step(2)
-        tuned = b.autotune(steps_per_trial=2)      # 10 shapes x (2 warm-up + 2 timed) steps
+        # 11 launches (10 tile-walk shapes and the per-case launch) x (2
+        # warm-up + 2 timed) steps
+        tuned = b.autotune(steps_per_trial=2)
         assert tuned["block"] in (128, 256) and tuned["blocks_per_sm"] in (0, 4, 8, 16, 32)
-        assert tuned["ms_per_step"] > 0
-        assert b.config()["block"] == tuned["block"]
+        assert tuned["ms_per_step"] > 0 and tuned["launch"] in ("tiles", "per_case")
+        assert b.config()["block"] == tuned["block"] and b.launch == tuned["launch"]
         b.step(2)
         total = cases[0].step_count
-        assert total == 2 + 2 + 40 + 2
+        assert total == 2 + 2 + 44 + 2
         got = states(cases)
     ref = make_cases(lbm, storage)
     for c in ref:
@@ -282,4 +284,74 @@ def test_batch_observables_equal_per_case(lbm, storage):
         for c, g in zip(rest, got):
             assert g == c.observables()
     for c in cases:
+        c.close()
+
+
+@pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "bf16s"])
+def test_per_case_launch_is_bitwise_lbm_step(lbm, storage):
+    """LBM_BATCH_PER_CASE launches each member's own single-case kernel, so
+    members end bitwise as lbm_step leaves them, in every storage format,
+    with mixed collision models, members joining at different step parities
+    (one in each AA layout), graphs of odd and even step counts, and a
+    switch back to the tile walk part-way."""
+    models = ["bgk", "regularized", "bgk", "bgk"]
+    solo = make_cases(lbm, storage)
+    for c, m in zip(solo, models):
+        c.set_collision(m)
+    solo[2].step(1)                            # one member starts in the other layout
+    for c in solo:
+        c.step(9)
+    want = states(solo)
+    cases = make_cases(lbm, storage)
+    for c, m in zip(cases, models):
+        c.set_collision(m)
+    cases[2].step(1)
+    with lbm.Batch(storage) as b:
+        b.set_launch("per_case")
+        assert b.launch == "per_case"
+        for c in cases:
+            b.add(c)
+        b.step(3)
+        b.step(1)
+        b.set_config(128, 0, use_graph=False)
+        b.step(2)
+        b.set_config(128, 0, use_graph=True)
+        b.set_launch("tiles")
+        b.step(2)
+        b.set_launch("per_case")
+        b.step(1)
+        got = states(cases)
+        obs = b.observables()
+    for i, (m, x, y) in enumerate(zip(models, want, got)):
+        for k in x:
+            if storage == "f32" or (storage in ("f16s", "bf16s") and m == "bgk"):
+                # the two tile-walk steps round as the batch kernel does
+                assert relerr(y[k], x[k]) <= {"f32": 2e-6, "f16s": 2e-3, "bf16s": 2e-2}[storage], (i, k)
+            else:
+                assert np.array_equal(x[k], y[k]), (i, m, k)
+    assert [o["step"] for o in obs] == [c.step_count for c in cases]
+    for c in solo + cases:
+        c.close()
+
+
+@pytest.mark.parametrize("storage", ["f32", "f16s"])
+def test_per_case_launch_alone_is_bitwise(lbm, storage):
+    """Without a tile-walk step in between, every member is bitwise the
+    single-case run in every format."""
+    solo = make_cases(lbm, storage)
+    for c in solo:
+        c.step(8)
+    want = states(solo)
+    cases = make_cases(lbm, storage)
+    with lbm.Batch(storage) as b:
+        b.set_launch("per_case")
+        for c in cases:
+            b.add(c)
+        b.step(5)
+        b.step(3)
+        got = states(cases)
+    for x, y in zip(want, got):
+        for k in x:
+            assert np.array_equal(x[k], y[k]), k
+    for c in solo + cases:
         c.close()
