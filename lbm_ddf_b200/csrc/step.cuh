@@ -334,6 +334,14 @@ __device__ __forceinline__ double mul_rn(double a, double b) { return __dmul_rn(
 __device__ __forceinline__ float fma_rn(float a, float b, float c) { return __fmaf_rn(a, b, c); }
 __device__ __forceinline__ double fma_rn(double a, double b, double c) { return __fma_rn(a, b, c); }
 
+// Paired FP32 operations (two lanes in one instruction on sm_100): each lane
+// rounds exactly as the scalar operation, so code written with them gives
+// the scalar code's bits.
+__device__ __forceinline__ float2 splat(float v) { return make_float2(v, v); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+
 // Regularised BGK (Latt and Chopard, Math. Comput. Simul. 72 (2006)
 // 165-168), an option beside the reference's BGK for relaxation times near
 // 1/2.  Same equilibria and force term as collide_fast; the non-equilibrium
@@ -635,47 +643,45 @@ template <class R> struct NodeOut {
 // update as collide_fast, with fewer instructions per node.
 
 template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
-__device__ __forceinline__ void gather_norm(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
+__device__ __forceinline__ void gather_norm(const A &a, const Node &g, float2 (&fg)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
-        const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
-        fh[K] = v.x;
-        gh[K] = v.y;
+        fg[K] = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
         // relative to the node's T_c; on interior rows of a periodic box in
         // the swapped layout the read and write re-referencing is folded
         // into the collision (collide_norm's `fold`), as the moments do not
         // see it (the deltas of each weight class sum to zero); a closed
         // box's x walls keep some populations in the node's own plane, so
         // there each delta is applied
-        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
     });
 }
 
-// gh here is g/w - s0 (s0 the node's conduction-profile temperature); t0 is
+// fg[i] = (fh_i, gh_i); gh here is g/w - s0 (s0 the node's conduction-profile temperature); t0 is
 // the mean temperature of the force term.
-__device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], const float (&gh)[Q], float phip,
-                                                       float gbeta, float t0, float s0) {
-    float r[4] = {0.f, 0.f, 0.f, 0.f}, x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f},
-          z[4] = {0.f, 0.f, 0.f, 0.f}, t[4] = {0.f, 0.f, 0.f, 0.f};
+__device__ __forceinline__ Moments<float> moments_norm(const float2 (&fg)[Q], float phip, float gbeta, float t0,
+                                                       float s0) {
+    float2 rt[4] = {};   // (sum fh, sum gh) per weight class, paired
+    float x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f}, z[4] = {0.f, 0.f, 0.f, 0.f};
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         constexpr int C = wclass(K);
-        r[C] += fh[K];
-        if (cx(K) > 0) x[C] += fh[K];
-        if (cx(K) < 0) x[C] -= fh[K];
-        if (cy(K) > 0) y[C] += fh[K];
-        if (cy(K) < 0) y[C] -= fh[K];
-        if (cz(K) > 0) z[C] += fh[K];
-        if (cz(K) < 0) z[C] -= fh[K];
-        t[C] += gh[K];
+        rt[C] = add2(rt[C], fg[K]);
+        if (cx(K) > 0) x[C] += fg[K].x;
+        if (cx(K) < 0) x[C] -= fg[K].x;
+        if (cy(K) > 0) y[C] += fg[K].x;
+        if (cy(K) < 0) y[C] -= fg[K].x;
+        if (cz(K) > 0) z[C] += fg[K].x;
+        if (cz(K) < 0) z[C] -= fg[K].x;
     });
     const float w0 = (float)wd(0), w1 = (float)wd(1), w2 = (float)wd(7), w3 = (float)wd(19);
     Moments<float> m;
-    m.rho = fmaf(w3, r[3], fmaf(w2, r[2], fmaf(w1, r[1], w0 * r[0])));
+    const float2 s = fma2(splat(w3), rt[3], fma2(splat(w2), rt[2], fma2(splat(w1), rt[1], mul2(splat(w0), rt[0]))));
+    m.rho = s.x;
     m.ux = fmaf(w3, x[3], fmaf(w2, x[2], w1 * x[1]));
     const float jy = fmaf(w3, y[3], fmaf(w2, y[2], w1 * y[1]));
     m.uz = fmaf(w3, z[3], fmaf(w2, z[2], w1 * z[1]));
-    m.phi = fmaf(w3, t[3], fmaf(w2, t[2], fmaf(w1, t[1], w0 * t[0]))) + s0;   // sum w_i (gh_i + s0)
+    m.phi = s.y + s0;   // sum w_i (gh_i + s0)
     m.uy = jy + 0.5f * (gbeta * (phip - t0));
     return m;
 }
@@ -691,9 +697,8 @@ __device__ __forceinline__ Moments<float> moments_norm(const float (&fh)[Q], con
 // were read from, and go to, the planes y - c_y and y + c_y (interior rows
 // of a periodic box, swapped layout): ag (v + c_y fold) + ... + c_y fold = ag v + ... +
 // (ag + 1) c_y fold, one more coefficient per c_y; else 0.
-__device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
-                                             float om_g, float force_fac, float gbeta, float t0, float s0,
-                                             float fold) {
+__device__ __forceinline__ void collide_norm(float2 (&fg)[Q], const Moments<float> &m, float om_f, float om_g,
+                                             float force_fac, float gbeta, float t0, float s0, float fold) {
     const float ux3 = 3.f * m.ux, uy3 = 3.f * m.uy, uz3 = 3.f * m.uz;
     const float uv = 3.f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
     const float kf = 3.f * force_fac * (gbeta * (m.phi - t0));
@@ -704,11 +709,12 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
     const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - s0);
     const float df = (ag + 1.f) * fold;
     const float d0c[3] = {d0 - df, d0, d0 + df};                    // indexed by c_y + 1
-    auto relax = [&](float &f, float &g, float p, int cy1) {
-        f = fmaf(af, f, fmaf(c1[cy1], p, c0[cy1]));
-        g = fmaf(ag, g, fmaf(d1, p, d0c[cy1]));
+    // (fh, gh) <- (af fh + c1 p + c0, ag gh + d1 p + d0c): both at once
+    const float2 a2 = make_float2(af, ag);
+    auto relax = [&](float2 &v, float p, int cy1) {
+        v = fma2(a2, v, fma2(make_float2(c1[cy1], d1), splat(p), make_float2(c0[cy1], d0c[cy1])));
     };
-    relax(fh[0], gh[0], -0.5f * uv, 1);
+    relax(fg[0], -0.5f * uv, 1);
     Unroll<1, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int J = opp(I);
@@ -721,8 +727,8 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
             if (cz(I) > 0) eu += uz3;
             if (cz(I) < 0) eu -= uz3;
             const float q = fmaf(eu, eu, -uv);
-            relax(fh[I], gh[I], fmaf(0.5f, q, eu), cy(I) + 1);
-            relax(fh[J], gh[J], fmaf(0.5f, q, -eu), cy(J) + 1);
+            relax(fg[I], fmaf(0.5f, q, eu), cy(I) + 1);
+            relax(fg[J], fmaf(0.5f, q, -eu), cy(J) + 1);
         }
     });
 }
@@ -731,19 +737,18 @@ __device__ __forceinline__ void collide_norm(float (&fh)[Q], float (&gh)[Q], con
 // form, gh' = 2 T_wall (1 + rho) - gh* - 2 t0, no weights on store, and one
 // 32-bit store of the packed (f, g) pair per population.
 template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
-__device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float (&fh)[Q], const float (&gh)[Q],
-                                             float rho, float s0) {
+__device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float2 (&fg)[Q], float rho, float s0) {
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
-        float gv = gh[I];
+        float gv = fg[I].y;
         const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
         const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
         // relative to T_c at the location written (folded into the
         // collision on interior rows of a periodic box's swapped layout)
         if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
-        const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
+        const typename Pack16<S>::T v = Pack16<S>::pack(fg[I].x, gv);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
             a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
         else
@@ -754,22 +759,22 @@ __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const fl
 template <class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t n) {
     const Node g = make_node<PERIODIC>(a, n);
-    float fh[Q], gh[Q];
+    float2 fg[Q];
     const bool interior = yz_interior<PERIODIC>(g);
     if (interior)
-        gather_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh);
+        gather_norm<S, SWAPPED, PERIODIC, true>(a, g, fg);
     else
-        gather_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh);
+        gather_norm<S, SWAPPED, PERIODIC, false>(a, g, fg);
     const float s0 = shift0(a, g);
-    Moments<float> m = moments_norm(fh, gh, a.phip[n], a.gb, a.t0, s0);
+    Moments<float> m = moments_norm(fg, a.phip[n], a.gb, a.t0, s0);
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_norm(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
+    collide_norm(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
                  SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
     a.phip[n] = m.phi;
     if (interior)
-        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
+        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fg, m.rho, s0);
     else
-        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho, s0);
+        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fg, m.rho, s0);
     return {m, g.iy};
 }
 
@@ -810,50 +815,47 @@ __host__ __device__ constexpr bool split_halves_ok() {
 static_assert(split_halves_ok(), "split update: bad population halves");
 
 template <int H, class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
-__device__ __forceinline__ void gather_half(const A &a, const Node &g, float (&fh)[Q], float (&gh)[Q]) {
+__device__ __forceinline__ void gather_half(const A &a, const Node &g, float2 (&fg)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if constexpr (half_of(K) == H) {
-            const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
-            fh[K] = v.x;
-            gh[K] = v.y;
-            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gh[K] += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+            fg[K] = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
+            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
         }
     });
 }
 
-// The half's share of rho, j_x, j_y, j_z and sum w_i gh_i (as moments_norm)
-template <int H>
-__device__ __forceinline__ void partial_moments(const float (&fh)[Q], const float (&gh)[Q], float (&p)[5]) {
-    float r[4] = {0.f, 0.f, 0.f, 0.f}, x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f},
-          z[4] = {0.f, 0.f, 0.f, 0.f}, t[4] = {0.f, 0.f, 0.f, 0.f};
+// The half's share of rho, j_x, j_y, j_z and sum w_i gh_i (as moments_norm);
+// the (rho, phi) class sums and their weighting as paired FP32 operations
+template <int H> __device__ __forceinline__ void partial_moments(const float2 (&fg)[Q], float (&p)[5]) {
+    float2 rt[4] = {};   // (sum fh, sum gh) per weight class
+    float x[4] = {0.f, 0.f, 0.f, 0.f}, y[4] = {0.f, 0.f, 0.f, 0.f}, z[4] = {0.f, 0.f, 0.f, 0.f};
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if constexpr (half_of(K) == H) {
             constexpr int C = wclass(K);
-            r[C] += fh[K];
-            if (cx(K) > 0) x[C] += fh[K];
-            if (cx(K) < 0) x[C] -= fh[K];
-            if (cy(K) > 0) y[C] += fh[K];
-            if (cy(K) < 0) y[C] -= fh[K];
-            if (cz(K) > 0) z[C] += fh[K];
-            if (cz(K) < 0) z[C] -= fh[K];
-            t[C] += gh[K];
+            rt[C] = add2(rt[C], fg[K]);
+            if (cx(K) > 0) x[C] += fg[K].x;
+            if (cx(K) < 0) x[C] -= fg[K].x;
+            if (cy(K) > 0) y[C] += fg[K].x;
+            if (cy(K) < 0) y[C] -= fg[K].x;
+            if (cz(K) > 0) z[C] += fg[K].x;
+            if (cz(K) < 0) z[C] -= fg[K].x;
         }
     });
     const float w0 = (float)wd(0), w1 = (float)wd(1), w2 = (float)wd(7), w3 = (float)wd(19);
-    p[0] = fmaf(w3, r[3], fmaf(w2, r[2], fmaf(w1, r[1], w0 * r[0])));
+    const float2 s = fma2(splat(w3), rt[3], fma2(splat(w2), rt[2], fma2(splat(w1), rt[1], mul2(splat(w0), rt[0]))));
+    p[0] = s.x;
     p[1] = fmaf(w3, x[3], fmaf(w2, x[2], w1 * x[1]));
     p[2] = fmaf(w3, y[3], fmaf(w2, y[2], w1 * y[1]));
     p[3] = fmaf(w3, z[3], fmaf(w2, z[2], w1 * z[1]));
-    p[4] = fmaf(w3, t[3], fmaf(w2, t[2], fmaf(w1, t[1], w0 * t[0])));
+    p[4] = s.y;
 }
 
 // collide_norm for the half's populations
 template <int H>
-__device__ __forceinline__ void collide_half(float (&fh)[Q], float (&gh)[Q], const Moments<float> &m, float om_f,
-                                             float om_g, float force_fac, float gbeta, float t0, float s0,
-                                             float fold) {
+__device__ __forceinline__ void collide_half(float2 (&fg)[Q], const Moments<float> &m, float om_f, float om_g,
+                                             float force_fac, float gbeta, float t0, float s0, float fold) {
     const float ux3 = 3.f * m.ux, uy3 = 3.f * m.uy, uz3 = 3.f * m.uz;
     const float uv = 3.f * (m.ux * m.ux + m.uy * m.uy + m.uz * m.uz);
     const float kf = 3.f * force_fac * (gbeta * (m.phi - t0));
@@ -864,11 +866,12 @@ __device__ __forceinline__ void collide_half(float (&fh)[Q], float (&gh)[Q], con
     const float ag = 1.f - om_g, d1 = om_g * m.phi, d0 = om_g * (m.phi - s0);
     const float df = (ag + 1.f) * fold;
     const float d0c[3] = {d0 - df, d0, d0 + df};
-    auto relax = [&](float &f, float &g, float p, int cy1) {
-        f = fmaf(af, f, fmaf(c1[cy1], p, c0[cy1]));
-        g = fmaf(ag, g, fmaf(d1, p, d0c[cy1]));
+    // (fh, gh) <- (af fh + c1 p + c0, ag gh + d1 p + d0c): both at once
+    const float2 a2 = make_float2(af, ag);
+    auto relax = [&](float2 &v, float p, int cy1) {
+        v = fma2(a2, v, fma2(make_float2(c1[cy1], d1), splat(p), make_float2(c0[cy1], d0c[cy1])));
     };
-    if constexpr (H == 0) relax(fh[0], gh[0], -0.5f * uv, 1);
+    if constexpr (H == 0) relax(fg[0], -0.5f * uv, 1);
     Unroll<1, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int J = opp(I);
@@ -881,26 +884,25 @@ __device__ __forceinline__ void collide_half(float (&fh)[Q], float (&gh)[Q], con
             if (cz(I) > 0) eu += uz3;
             if (cz(I) < 0) eu -= uz3;
             const float q = fmaf(eu, eu, -uv);
-            relax(fh[I], gh[I], fmaf(0.5f, q, eu), cy(I) + 1);
-            relax(fh[J], gh[J], fmaf(0.5f, q, -eu), cy(J) + 1);
+            relax(fg[I], fmaf(0.5f, q, eu), cy(I) + 1);
+            relax(fg[J], fmaf(0.5f, q, -eu), cy(J) + 1);
         }
     });
 }
 
 // scatter_norm for the half's populations
 template <int H, class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
-__device__ __forceinline__ void scatter_half(const A &a, const Node &g, const float (&fh)[Q], const float (&gh)[Q],
-                                             float rho, float s0) {
+__device__ __forceinline__ void scatter_half(const A &a, const Node &g, const float2 (&fg)[Q], float rho, float s0) {
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         if constexpr (half_of(I) == H) {
             constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
-            float gv = gh[I];
+            float gv = fg[I].y;
             const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
             const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
             if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
             if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
-            const typename Pack16<S>::T v = Pack16<S>::pack(fh[I], gv);
+            const typename Pack16<S>::T v = Pack16<S>::pack(fg[I].x, gv);
             if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
                 a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
             else
@@ -925,7 +927,7 @@ __device__ __forceinline__ void pair_barrier(int pair) {
 template <int H, class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid, float (&xch)[2][5][32], int lane,
                                              int pair) {
-    float fh[Q], gh[Q];
+    float2 fg[Q];
     float p[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     Node g{};
     bool interior = false;
@@ -935,10 +937,10 @@ __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid,
         g = make_node<PERIODIC>(a, n);
         interior = yz_interior<PERIODIC>(g);
         if (interior)
-            gather_half<H, S, SWAPPED, PERIODIC, true>(a, g, fh, gh);
+            gather_half<H, S, SWAPPED, PERIODIC, true>(a, g, fg);
         else
-            gather_half<H, S, SWAPPED, PERIODIC, false>(a, g, fh, gh);
-        partial_moments<H>(fh, gh, p);
+            gather_half<H, S, SWAPPED, PERIODIC, false>(a, g, fg);
+        partial_moments<H>(fg, p);
     }
 #pragma unroll
     for (int i = 0; i < 5; i++) xch[H][i][lane] = p[i];
@@ -955,13 +957,13 @@ __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid,
     m.uz = tot[3];
     m.phi = tot[4] + s0;
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_half<H>(fh, gh, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
+    collide_half<H>(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
                     SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
     if (H == 0) a.phip[n] = m.phi;
     if (interior)
-        scatter_half<H, S, SWAPPED, PERIODIC, true>(a, g, fh, gh, m.rho, s0);
+        scatter_half<H, S, SWAPPED, PERIODIC, true>(a, g, fg, m.rho, s0);
     else
-        scatter_half<H, S, SWAPPED, PERIODIC, false>(a, g, fh, gh, m.rho, s0);
+        scatter_half<H, S, SWAPPED, PERIODIC, false>(a, g, fg, m.rho, s0);
 }
 
 template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A>
