@@ -312,9 +312,30 @@ void launch_group(const BatchCase<S> *cases, int n, const uint32_t *start, bool 
     else batch_step_kernel<S, BLOCK, SW, LBM_COLLISION_BGK><<<grid, BLOCK, 0, st>>>(cases, n, start);
 }
 
+// Lane of each member for the per-case launch: members by decreasing node
+// count, each onto the lane with the fewest nodes so far (longest processing
+// time first), so the lanes' work is balanced.  A lane runs its members'
+// steps in order, and the lanes of a captured multi-step graph progress
+// independently, so the slowest lane sets the time.
+std::vector<int> lane_of_members(const lbm_batch *b, int lanes) {
+    const size_t n = b->members.size();
+    std::vector<size_t> order(n);
+    for (size_t i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](size_t x, size_t y) { return b->members[x]->nodes > b->members[y]->nodes; });
+    std::vector<int64_t> load((size_t)lanes, 0);
+    std::vector<int> lane(n, 0);
+    for (size_t i : order) {
+        const int l = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        lane[i] = l;
+        load[(size_t)l] += b->members[i]->nodes;
+    }
+    return lane;
+}
+
 // LBM_BATCH_PER_CASE: `nsteps` steps of every member, each through its own
 // single-case node kernel (its parameters in the constant bank, as lbm_step
-// launches it), member i on lane i mod kLanes; the lanes are forked from
+// launches it), on the lanes of lane_of_members; the lanes are forked from
 // and joined to `st` by events, so captured into a graph the members' steps
 // are parallel branches and the kernels of different members run
 // concurrently.
@@ -327,12 +348,13 @@ int enqueue_steps_per_case(lbm_batch *b, int nsteps, cudaStream_t st) {
         }
     }
     const int nl = std::min<int>(kLanes, (int)b->members.size());
+    const std::vector<int> lane = lane_of_members(b, nl);
     CUDA_TRY(cudaEventRecord(b->fork_ev, st));
     for (int l = 0; l < nl; l++) CUDA_TRY(cudaStreamWaitEvent(b->lanes[l], b->fork_ev, 0));
     for (int s = 0; s < nsteps; s++)
         for (size_t i = 0; i < b->members.size(); i++) {
             const lbm_case *c = b->members[i];
-            const int rc = enqueue_case_step(c, c->swapped != ((s & 1) != 0), b->lanes[i % kLanes]);
+            const int rc = enqueue_case_step(c, c->swapped != ((s & 1) != 0), b->lanes[lane[i]]);
             if (rc) return rc;
         }
     for (int l = 0; l < nl; l++) {
