@@ -232,12 +232,11 @@ int lbm_selfcheck_division(int device, double divisor, uint64_t n, uint64_t seed
 /* Advances nsteps steps and returns, in out[0 .. nsteps) (host memory), the
  * observables of every state the steps started from: out[i] is the state
  * after (initial step count + i) steps, as lbm_get_observables would report
- * it then.  For FP64 and FP32 storage each step kernel reduces them from
- * the moments it computes anyway, so the per-step observables cost no extra
- * read of the state (lbm_get_observables reads all populations once); for
- * 16-bit storage, whose step is issue-bound, a separate reduction before
- * each step measured faster and is used.  Call lbm_get_observables for the
- * state after the last step.  Node kernel only
+ * it then.  Each step kernel reduces them from the moments it computes
+ * anyway (in every storage format; for 16-bit BGK, half of each warp pair
+ * of the split kernel), so the per-step observables cost no extra read of
+ * the state (lbm_get_observables reads all populations once).  Call
+ * lbm_get_observables for the state after the last step.  Node kernel only
  * (LBM_ERR_ARG if the case's step kernel is set to ROW); synchronises
  * `stream`; LBM_ERR_DIVERGED if any entry saw a NaN/Inf (all entries are
  * written).  The sums' order differs from lbm_get_observables', so results

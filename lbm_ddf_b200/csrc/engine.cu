@@ -70,22 +70,33 @@ namespace lbm {
 //   6..8  phi on the planes iy = 0, 1, 2
 //   9..11 phi on the planes iy = LY-1, LY-2, LY-3
 //   12 number of nodes with a non-finite moment
+//
+// split: the moments as the 16-bit BGK step kernel forms them (split_moments),
+// so these observables match those it reduces when it steps; else as the
+// node update forms them.
 template <class S, bool SWAPPED, bool PERIODIC>
-__global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, double *__restrict__ partial) {
+__global__ void __launch_bounds__(kObsThreads) obs_kernel(const StepArgs<S> a, double *__restrict__ partial,
+                                                          int split) {
     using R = typename Codec<S>::R;
     double acc[kObs];
 #pragma unroll
     for (int k = 0; k < kObs; k++) acc[k] = 0.0;
     for (uint32_t n = blockIdx.x * blockDim.x + threadIdx.x; n < a.nodes; n += gridDim.x * blockDim.x) {
         const Node g = make_node<PERIODIC>(a, n);
+        if constexpr (elem_stride<S>() == 2) {
+            if (split) {
+                add_obs_terms(acc, split_moments<S, SWAPPED, PERIODIC>(a, g), g.iy, a.ly);
+                continue;
+            }
+        }
         R fr[Q], gr[Q];
         // rows away from the plates (and a closed box's z walls): no y or z
         // boundary tests (uniform over a warp whenever LX is a multiple of
         // 32); FP64 keeps one path (two do not fit its registers)
         if (sizeof(S) < 8 && SWAPPED && yz_interior<PERIODIC>(g))
-            gather<S, SWAPPED, true>(a, g, fr, gr);
+            gather<S, SWAPPED, kRowInside>(a, g, fr, gr);
         else
-            gather<S, SWAPPED, false>(a, g, fr, gr);
+            gather<S, SWAPPED, kNoneInside>(a, g, fr, gr);
         const Moments<R> m = node_moments<S>(a, fr, gr, n);
         add_obs_terms(acc, m, g.iy, a.ly);
     }
@@ -219,7 +230,7 @@ __global__ void export_pop_kernel(const StepArgs<S> a, int which, int k, double 
             // 16-bit storage: g/w is stored relative to the conduction
             // profile at the location read (step.cuh shift0)
             float sh = 0.f;
-            if constexpr (elem_stride<S>() == 2) sh = shift0(a, g) + read_shift_delta<SWAPPED, K, false>(a, g);
+            if constexpr (elem_stride<S>() == 2) sh = shift0(a, g) + read_shift_delta<SWAPPED, K, kNoneInside>(a, g);
             if (which)
                 v = (double)C::template g_in<K>(load_pop<S, SWAPPED, K, false, 1>(a, g),
                                                 elem_stride<S>() == 2 ? (typename C::R)sh : a.t0);
@@ -449,12 +460,17 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
     return fail(LBM_ERR_ARG, "bad storage");
 }
 
+// Whether the case steps on step16_split_kernel (16-bit storage, BGK): 64
+// nodes per block there, 128 in step_kernel.
+bool split_step(const lbm_case *c) { return interleaved(c) && c->collision == LBM_COLLISION_BGK; }
+int step_blocks(const lbm_case *c) { return (int)grid_for(c->nodes, split_step(c) ? 64 : kStepThreads); }
+
 template <class S, bool SW, bool PER, bool OBS = false>
 void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
     // 16-bit storage, BGK: one node's update split over two warps
-    if constexpr (sizeof(S) == 2 && !OBS) {
+    if constexpr (sizeof(S) == 2) {
         if (c->collision == LBM_COLLISION_BGK) {
-            step16_split_kernel<S, SW, PER><<<grid_for(c->nodes, 64), 128, 0, st>>>(a);
+            step16_split_kernel<S, SW, PER, OBS><<<grid_for(c->nodes, 64), 128, 0, st>>>(a);
             return;
         }
     }
@@ -468,7 +484,6 @@ void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
 // One node-kernel step that also writes the observables of the state it
 // reads as per-block rows into a.obs_rows.
 template <class S> void launch_step_observed(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
-    static_assert(sizeof(S) > 2, "16-bit steps reduce their observables in a separate pass");
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
         if (per) launch_step_t<S, true, true, true>(c, a, st);
@@ -833,7 +848,7 @@ int lbm_internal::enqueue_observables(const lbm_case *c, lbm_observables *dst, c
     return with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const StepArgs<S> a = make_args<S>(c);
-        LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
+        LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial, split_step(c) ? 1 : 0);
         ObsConsts k;
         k.nodes = (double)c->nodes;
         k.plane = (double)c->p.lx * (double)c->p.lz;
@@ -899,10 +914,14 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
     if (nsteps == 0) return LBM_OK;
     DeviceGuard dg(c->p.device);
     cudaStream_t st = (cudaStream_t)stream;
-    const int rows = (int)grid_for(c->nodes, kStepThreads);
+    // one row per step-kernel block: room for the 64-node blocks of the
+    // 16-bit BGK kernel, whichever kernel the case uses now
+    const int rows = step_blocks(c);
     const int parts = (rows + kRowChunk - 1) / kRowChunk;
+    const int max_rows = (int)grid_for(c->nodes, 64);
+    const int max_parts = (max_rows + kRowChunk - 1) / kRowChunk;
     if (!c->obs_rows) {   // per-block rows, then the chunk partials behind them
-        CUDA_TRY(cudaMalloc(&c->obs_rows, (size_t)(rows + parts) * kObs * sizeof(double)));
+        CUDA_TRY(cudaMalloc(&c->obs_rows, (size_t)(max_rows + max_parts) * kObs * sizeof(double)));
     }
     if (nsteps > c->obs_series_cap) {
         if (c->obs_series) {
@@ -914,7 +933,7 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
         CUDA_TRY(cudaMalloc(&c->obs_series, (size_t)nsteps * sizeof(lbm_observables)));
         c->obs_series_cap = nsteps;
     }
-    double *partial = c->obs_rows + (size_t)rows * kObs;
+    double *partial = c->obs_rows + (size_t)max_rows * kObs;
     rc = with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         StepArgs<S> a = make_args<S>(c);
@@ -928,18 +947,9 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
         k.visc = c->d.visc;
         for (int s = 0; s < nsteps; s++) {
             k.step = c->step + s;   // the state this step starts from
-            if constexpr (sizeof(S) == 2) {
-                // 16-bit storage: the step is issue-bound, and folding the
-                // reduction into it cost more (B200, 256^3: +0.43 ms per
-                // step) than a separate pass over the state (0.30-0.40 ms)
-                LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial);
-                obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, c->obs_series + s);
-                (void)launch_step<S>(c, a, st);   // a launch error is read after the loop
-            } else {
-                launch_step_observed<S>(c, a, st);
-                obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial);
-                obs_finalize<<<1, 32 * kObs, 0, st>>>(partial, parts, k, c->obs_series + s);
-            }
+            launch_step_observed<S>(c, a, st);
+            obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial);
+            obs_finalize<<<1, 32 * kObs, 0, st>>>(partial, parts, k, c->obs_series + s);
             c->swapped = !c->swapped;
             c->rest_phi = false;
             a.use_phi_fix = 0;
@@ -1158,7 +1168,8 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
         using S = std::remove_pointer_t<decltype(tag)>;
         const StepArgs<S> a = make_args<S>(&view);
         const lbm_case *c = &view;
-        LBM_DISPATCH_LAYOUT(c, obs_kernel, blocks, kObsThreads, st, a, scratch);
+        // 16-bit storage: the moments as the BGK step kernel forms them
+        LBM_DISPATCH_LAYOUT(c, obs_kernel, blocks, kObsThreads, st, a, scratch, interleaved(c) ? 1 : 0);
         ObsConsts k;
         k.nodes = (double)nodes;
         k.plane = (double)p->lx * (double)p->lz;

@@ -167,15 +167,28 @@ __device__ __forceinline__ bool inside(const Node &g) {
     return (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) && (DY < 0 ? g.vym : DY > 0 ? g.vyp : true) &&
            (DZ < 0 ? g.vzm : DZ > 0 ? g.vzp : true);
 }
-// With INTERIOR set the caller guarantees that the neighbours along y and z
-// are inside the box (0 < iy < LY-1, and periodic sides or 0 < iz < LZ-1),
-// so only the x neighbour is tested (a compile-time true with periodic
-// sides; a per-lane select at the x walls of a closed box, where the node's
-// warp still takes this path, since a warp lies in one row when LX is a
-// multiple of 32).
-template <bool INTERIOR, int DX, int DY, int DZ>
+// Which neighbours a node update may take as inside the box without a test
+// (the INTERIOR template argument of the gathers and scatters):
+//   kNoneInside: none, every neighbour is tested;
+//   kRowInside:  those along y and z (0 < iy < LY-1, and periodic sides or
+//                0 < iz < LZ-1): only the x neighbour is tested, which is a
+//                compile-time true with periodic sides and a per-lane select
+//                at the x walls of a closed box;
+//   kAllInside:  all of them (a closed box's rows whose warp holds no x-wall
+//                node: with LX a multiple of 32, all but the first and last
+//                warp of a row).
+constexpr int kNoneInside = 0, kRowInside = 1, kAllInside = 2;
+template <int INTERIOR, int DX, int DY, int DZ>
 __device__ __forceinline__ bool inside_t(const Node &g) {
-    return INTERIOR ? (DX < 0 ? g.vxm : DX > 0 ? g.vxp : true) : inside<DX, DY, DZ>(g);
+    if constexpr (INTERIOR == kAllInside) return true;
+    else if constexpr (INTERIOR == kRowInside) return DX < 0 ? g.vxm : DX > 0 ? g.vxp : true;
+    else return inside<DX, DY, DZ>(g);
+}
+// whether every neighbour of a node taking this path is inside (so the
+// swapped layout reads every population from, and writes it to, the
+// neighbouring planes: the 16-bit update's plane-shift fold applies)
+template <int INTERIOR, bool PERIODIC> constexpr bool all_inside() {
+    return INTERIOR == kAllInside || (INTERIOR == kRowInside && PERIODIC);
 }
 
 // Whether node g's neighbours along y and z are all inside the box (the
@@ -185,9 +198,21 @@ template <bool PERIODIC> __device__ __forceinline__ bool yz_interior(const Node 
     return g.vym && g.vyp && (PERIODIC || (g.vzm && g.vzp));
 }
 
+// The path of node g's update (the INTERIOR argument, see inside_t):
+// kRowInside for rows whose y and z neighbours are inside, kAllInside for
+// those of a closed box when no active lane of the warp lies at an x wall
+// (decided over the warp, so a warp takes one path), else kNoneInside.
+template <bool PERIODIC> __device__ __forceinline__ int node_path(const Node &g) {
+    if (!yz_interior<PERIODIC>(g)) return kNoneInside;
+    if constexpr (!PERIODIC) {
+        if (__all_sync(__activemask(), g.vxm && g.vxp)) return kAllInside;
+    }
+    return kRowInside;
+}
+
 // Population k (of f when WHICH = 0, of g when 1) of node g at the current
 // time, from either layout.  `a` supplies the addresses: a.ld(which, k, node).
-template <class S, bool SWAPPED, int K, bool INTERIOR = false, int WHICH = 0, class A>
+template <class S, bool SWAPPED, int K, int INTERIOR = kNoneInside, int WHICH = 0, class A>
 __device__ __forceinline__ S load_pop(const A &a, const Node &g) {
     if (!SWAPPED) return a.ld(WHICH, K, g.n);
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
@@ -197,7 +222,7 @@ __device__ __forceinline__ S load_pop(const A &a, const Node &g) {
 
 // The (f_k, g_k) pair that node g collides in this step, as load_pop finds
 // each value, with one 32-bit load.
-template <class S, bool SWAPPED, int K, bool INTERIOR, class A>
+template <class S, bool SWAPPED, int K, int INTERIOR, class A>
 __device__ __forceinline__ typename Pack16<S>::T load_pair(const A &a, const Node &g) {
     if (!SWAPPED) return a.ld2(K, g.n);
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
@@ -221,20 +246,20 @@ __device__ __forceinline__ typename Pack16<S>::T load_pair(const A &a, const Nod
 template <class A> __device__ __forceinline__ float shift0(const A &a, const Node &g) {
     return fmaf(-(float)g.iy, (float)a.t_dy, (float)a.t_top);
 }
-template <bool SWAPPED, int K, bool INTERIOR, class A>
+template <bool SWAPPED, int K, int INTERIOR, class A>
 __device__ __forceinline__ float read_shift_delta(const A &a, const Node &g) {
     constexpr int DX = -cx(K), DY = -cy(K), DZ = -cz(K);
     if constexpr (!SWAPPED || DY == 0) return 0.f;
     else return inside_t<INTERIOR, DX, DY, DZ>(g) ? (float)cy(K) * (float)a.t_dy : 0.f;
 }
-template <bool SWAPPED, int I, bool INTERIOR, class A>
+template <bool SWAPPED, int I, int INTERIOR, class A>
 __device__ __forceinline__ float write_shift_delta(const A &a, const Node &g) {
     constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
     if constexpr (!SWAPPED || DY == 0) return 0.f;
     else return inside_t<INTERIOR, DX, DY, DZ>(g) ? (float)cy(I) * (float)a.t_dy : 0.f;
 }
 
-template <class S, bool SWAPPED, bool INTERIOR = false, class A>
+template <class S, bool SWAPPED, int INTERIOR = kNoneInside, class A>
 __device__ __forceinline__ void gather(const A &a, const Node &g, typename Codec<S>::R (&fr)[Q],
                                        typename Codec<S>::R (&gr)[Q]) {
     using C = Codec<S>;
@@ -243,9 +268,13 @@ __device__ __forceinline__ void gather(const A &a, const Node &g, typename Codec
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: f_i = w_i fh, g_i = w_i (gh + T_c at the location)
+            // explicit rounding: the compiler cannot fuse these products into
+            // the moment sums in one kernel and not in another, so every
+            // kernel that gathers (the step, the observables) forms the same
+            // FP32 moments
             const float2 v = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
-            fr[K] = (float)wd(K) * v.x;
-            gr[K] = (float)wd(K) * (v.y + (s0 + read_shift_delta<SWAPPED, K, INTERIOR>(a, g)));
+            fr[K] = __fmul_rn((float)wd(K), v.x);
+            gr[K] = __fmul_rn((float)wd(K), __fadd_rn(v.y, __fadd_rn(s0, read_shift_delta<SWAPPED, K, INTERIOR>(a, g))));
         } else {
             fr[K] = C::template f_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 0>(a, g), a.t0);
             gr[K] = C::template g_in<K>(load_pop<S, SWAPPED, K, INTERIOR, 1>(a, g), a.t0);
@@ -276,7 +305,10 @@ __device__ __forceinline__ Moments<R> moments(const R (&fr)[Q], const R (&gr)[Q]
     });
     m.rho = rho;
     m.ux = jx;
-    m.uy = jy + R(0.5) * (gb * (phip - t0));
+    if constexpr (std::is_same<R, float>::value)   // explicit rounding: the same in every kernel
+        m.uy = __fadd_rn(jy, __fmul_rn(0.5f, __fmul_rn(gb, __fsub_rn(phip, t0))));
+    else   // FP64: as written, the rounding the reference build has (bitwise parity)
+        m.uy = jy + R(0.5) * (gb * (phip - t0));
     m.uz = jz;
     m.phi = phi;
     return m;
@@ -503,7 +535,7 @@ __device__ __forceinline__ R abb(R gv, R tw, R rho) {
 
 // Write the post-collision populations of node g to where the next step
 // reads them.  rho is the node's pre-collision density (for anti-bounce-back).
-template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR = false, class A>
+template <class S, bool SWAPPED, bool PERIODIC, int INTERIOR = kNoneInside, class A>
 __device__ __forceinline__ void scatter(const A &a, const Node &g, const typename Codec<S>::R (&fr)[Q],
                                         const typename Codec<S>::R (&gr)[Q], typename Codec<S>::R rho) {
     using C = Codec<S>;
@@ -515,8 +547,8 @@ __device__ __forceinline__ void scatter(const A &a, const Node &g, const typenam
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
         R fv = fr[I];
         R gv = gr[I];
-        const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-        const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        const bool out_y = INTERIOR == kNoneInside && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
+        const bool out_z = !PERIODIC && INTERIOR == kNoneInside && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = abb<I>(gv, DY < 0 ? a.t_hot : a.t_cold, rho);
         if constexpr (elem_stride<S>() == 2) {   // (f, g) pairs: f/w and g/w - T_c at the location, packed
             // the location's T_c is s0 - write_shift_delta (it is s0 at the node itself)
@@ -642,7 +674,7 @@ template <class R> struct NodeOut {
 // Opposite directions share c.u and the quadratic part of p.  The same
 // update as collide_fast, with fewer instructions per node.
 
-template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
+template <class S, bool SWAPPED, bool PERIODIC, int INTERIOR, class A>
 __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float2 (&fg)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
@@ -653,7 +685,7 @@ __device__ __forceinline__ void gather_norm(const A &a, const Node &g, float2 (&
         // see it (the deltas of each weight class sum to zero); a closed
         // box's x walls keep some populations in the node's own plane, so
         // there each delta is applied
-        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+        if constexpr (!(SWAPPED && all_inside<INTERIOR, PERIODIC>())) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
     });
 }
 
@@ -736,18 +768,18 @@ __device__ __forceinline__ void collide_norm(float2 (&fg)[Q], const Moments<floa
 // scatter() for the normalised variables: anti-bounce-back in normalised
 // form, gh' = 2 T_wall (1 + rho) - gh* - 2 t0, no weights on store, and one
 // 32-bit store of the packed (f, g) pair per population.
-template <class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
+template <class S, bool SWAPPED, bool PERIODIC, int INTERIOR, class A>
 __device__ __forceinline__ void scatter_norm(const A &a, const Node &g, const float2 (&fg)[Q], float rho, float s0) {
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
         float gv = fg[I].y;
-        const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-        const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+        const bool out_y = INTERIOR == kNoneInside && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
+        const bool out_z = !PERIODIC && INTERIOR == kNoneInside && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
         if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
         // relative to T_c at the location written (folded into the
         // collision on interior rows of a periodic box's swapped layout)
-        if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
+        if constexpr (!(SWAPPED && all_inside<INTERIOR, PERIODIC>())) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
         const typename Pack16<S>::T v = Pack16<S>::pack(fg[I].x, gv);
         if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
             a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -760,21 +792,25 @@ template <class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t n) {
     const Node g = make_node<PERIODIC>(a, n);
     float2 fg[Q];
-    const bool interior = yz_interior<PERIODIC>(g);
-    if (interior)
-        gather_norm<S, SWAPPED, PERIODIC, true>(a, g, fg);
+    const int path = node_path<PERIODIC>(g);
+    if (path == kRowInside)
+        gather_norm<S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
+    else if (!PERIODIC && path == kAllInside)
+        gather_norm<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
     else
-        gather_norm<S, SWAPPED, PERIODIC, false>(a, g, fg);
+        gather_norm<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
     const float s0 = shift0(a, g);
     Moments<float> m = moments_norm(fg, a.phip[n], a.gb, a.t0, s0);
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_norm(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
-                 SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
+    const bool fold = SWAPPED && (path == kAllInside || (PERIODIC && path == kRowInside));
+    collide_norm(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0, fold ? (float)a.t_dy : 0.f);
     a.phip[n] = m.phi;
-    if (interior)
-        scatter_norm<S, SWAPPED, PERIODIC, true>(a, g, fg, m.rho, s0);
+    if (path == kRowInside)
+        scatter_norm<S, SWAPPED, PERIODIC, kRowInside>(a, g, fg, m.rho, s0);
+    else if (!PERIODIC && path == kAllInside)
+        scatter_norm<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg, m.rho, s0);
     else
-        scatter_norm<S, SWAPPED, PERIODIC, false>(a, g, fg, m.rho, s0);
+        scatter_norm<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg, m.rho, s0);
     return {m, g.iy};
 }
 
@@ -814,13 +850,13 @@ __host__ __device__ constexpr bool split_halves_ok() {
 }
 static_assert(split_halves_ok(), "split update: bad population halves");
 
-template <int H, class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
+template <int H, class S, bool SWAPPED, bool PERIODIC, int INTERIOR, class A>
 __device__ __forceinline__ void gather_half(const A &a, const Node &g, float2 (&fg)[Q]) {
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
         if constexpr (half_of(K) == H) {
             fg[K] = Pack16<S>::unpack(load_pair<S, SWAPPED, K, INTERIOR>(a, g));
-            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
+            if constexpr (!(SWAPPED && all_inside<INTERIOR, PERIODIC>())) fg[K].y += read_shift_delta<SWAPPED, K, INTERIOR>(a, g);
         }
     });
 }
@@ -891,17 +927,17 @@ __device__ __forceinline__ void collide_half(float2 (&fg)[Q], const Moments<floa
 }
 
 // scatter_norm for the half's populations
-template <int H, class S, bool SWAPPED, bool PERIODIC, bool INTERIOR, class A>
+template <int H, class S, bool SWAPPED, bool PERIODIC, int INTERIOR, class A>
 __device__ __forceinline__ void scatter_half(const A &a, const Node &g, const float2 (&fg)[Q], float rho, float s0) {
     Unroll<0, Q>::run([&](auto ii) {
         constexpr int I = decltype(ii)::value;
         if constexpr (half_of(I) == H) {
             constexpr int DX = cx(I), DY = cy(I), DZ = cz(I);
             float gv = fg[I].y;
-            const bool out_y = !INTERIOR && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
-            const bool out_z = !PERIODIC && !INTERIOR && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
+            const bool out_y = INTERIOR == kNoneInside && ((DY < 0 && !g.vym) || (DY > 0 && !g.vyp));
+            const bool out_z = !PERIODIC && INTERIOR == kNoneInside && ((DZ < 0 && !g.vzm) || (DZ > 0 && !g.vzp));
             if (DY != 0 && out_y && !out_z) gv = 2.f * (DY < 0 ? a.t_hot : a.t_cold) * (1.f + rho) - gv - 2.f * s0;
-            if constexpr (!(INTERIOR && SWAPPED && PERIODIC)) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
+            if constexpr (!(SWAPPED && all_inside<INTERIOR, PERIODIC>())) gv += write_shift_delta<SWAPPED, I, INTERIOR>(a, g);
             const typename Pack16<S>::T v = Pack16<S>::pack(fg[I].x, gv);
             if (SWAPPED && inside_t<INTERIOR, DX, DY, DZ>(g))
                 a.st2(I, (int32_t)g.n + disp<DX, DY, DZ>(g)) = v;
@@ -924,28 +960,32 @@ __device__ __forceinline__ void pair_barrier(int pair) {
 // Half H of the update of node n (valid: n is a node); xch is the warp
 // pair's exchange area [half][moment][lane].  Both warps of a pair call it
 // once, valid or not, and pass the barrier once.
+// Returns the node's moments (those of the state it read) and plane; they
+// are meaningful for valid nodes only.
 template <int H, class S, bool SWAPPED, bool PERIODIC, class A>
-__device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid, float (&xch)[2][5][32], int lane,
-                                             int pair) {
+__device__ __forceinline__ NodeOut<float> split_update(const A &a, uint32_t n, bool valid, float (&xch)[2][5][32],
+                                                       int lane, int pair) {
     float2 fg[Q];
     float p[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     Node g{};
-    bool interior = false;
+    int path = kNoneInside;
     float phip = 0.f;
     if (valid) {
         phip = a.phip[n];   // before the barrier: half 0 overwrites it after
         g = make_node<PERIODIC>(a, n);
-        interior = yz_interior<PERIODIC>(g);
-        if (interior)
-            gather_half<H, S, SWAPPED, PERIODIC, true>(a, g, fg);
+        path = node_path<PERIODIC>(g);
+        if (path == kRowInside)
+            gather_half<H, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
+        else if (!PERIODIC && path == kAllInside)
+            gather_half<H, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
         else
-            gather_half<H, S, SWAPPED, PERIODIC, false>(a, g, fg);
+            gather_half<H, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
         partial_moments<H>(fg, p);
     }
 #pragma unroll
     for (int i = 0; i < 5; i++) xch[H][i][lane] = p[i];
     pair_barrier(pair);
-    if (!valid) return;
+    if (!valid) return {};
     float tot[5];
 #pragma unroll
     for (int i = 0; i < 5; i++) tot[i] = p[i] + xch[1 - H][i][lane];
@@ -953,17 +993,51 @@ __device__ __forceinline__ void split_update(const A &a, uint32_t n, bool valid,
     Moments<float> m;
     m.rho = tot[0];
     m.ux = tot[1];
-    m.uy = tot[2] + 0.5f * (a.gb * (phip - a.t0));
+    m.uy = __fadd_rn(tot[2], __fmul_rn(0.5f, __fmul_rn(a.gb, __fsub_rn(phip, a.t0))));   // as split_moments
     m.uz = tot[3];
     m.phi = tot[4] + s0;
     if (a.use_phi_fix) m.phi = a.phi_fix;
-    collide_half<H>(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0,
-                    SWAPPED && PERIODIC && interior ? (float)a.t_dy : 0.f);
+    const bool fold = SWAPPED && (path == kAllInside || (PERIODIC && path == kRowInside));
+    collide_half<H>(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0, fold ? (float)a.t_dy : 0.f);
     if (H == 0) a.phip[n] = m.phi;
-    if (interior)
-        scatter_half<H, S, SWAPPED, PERIODIC, true>(a, g, fg, m.rho, s0);
+    if (path == kRowInside)
+        scatter_half<H, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg, m.rho, s0);
+    else if (!PERIODIC && path == kAllInside)
+        scatter_half<H, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg, m.rho, s0);
     else
-        scatter_half<H, S, SWAPPED, PERIODIC, false>(a, g, fg, m.rho, s0);
+        scatter_half<H, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg, m.rho, s0);
+    return {m, g.iy};
+}
+
+// The moments of node g exactly as step16_split_kernel's two halves form
+// them (the same loads on the same path, the same partial sums, added in the
+// same order), so observables reduced from them match those the kernel
+// reduces when it steps (the observables of its OBS variant).
+template <class S, bool SWAPPED, bool PERIODIC, class A>
+__device__ __forceinline__ Moments<float> split_moments(const A &a, const Node &g) {
+    float2 fg[Q];
+    float p0[5], p1[5];
+    const int path = node_path<PERIODIC>(g);
+    if (path == kRowInside) {
+        gather_half<0, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
+        gather_half<1, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
+    } else if (!PERIODIC && path == kAllInside) {
+        gather_half<0, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
+        gather_half<1, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
+    } else {
+        gather_half<0, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
+        gather_half<1, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
+    }
+    partial_moments<0>(fg, p0);
+    partial_moments<1>(fg, p1);
+    Moments<float> m;
+    m.rho = p0[0] + p1[0];
+    m.ux = p0[1] + p1[1];
+    m.uy = __fadd_rn(p0[2] + p1[2], __fmul_rn(0.5f, __fmul_rn(a.gb, __fsub_rn((float)a.phip[g.n], a.t0))));
+    m.uz = p0[3] + p1[3];
+    m.phi = (p0[4] + p1[4]) + shift0(a, g);
+    if (a.use_phi_fix) m.phi = a.phi_fix;
+    return m;
 }
 
 template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A>
@@ -975,20 +1049,25 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     // Rows away from the plates (and, in a closed box, from the z walls)
-    // need no y or z boundary tests; the branch is uniform over a warp
-    // whenever LX is a multiple of 32.
-    const bool interior = yz_interior<PERIODIC>(g);
-    if (interior)
-        gather<S, SWAPPED, true>(a, g, fr, gr);
+    // need no y or z boundary tests, and a closed box's warps with no x-wall
+    // node none at all; the path is uniform over a warp whenever LX is a
+    // multiple of 32.
+    const int path = node_path<PERIODIC>(g);
+    if (path == kRowInside)
+        gather<S, SWAPPED, kRowInside>(a, g, fr, gr);
+    else if (!PERIODIC && path == kAllInside)
+        gather<S, SWAPPED, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr);
     else
-        gather<S, SWAPPED, false>(a, g, fr, gr);
+        gather<S, SWAPPED, kNoneInside>(a, g, fr, gr);
     const Moments<R> m = node_moments<S>(a, fr, gr, n);
     collide<S, COLL>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
-    if (interior)
-        scatter<S, SWAPPED, PERIODIC, true>(a, g, fr, gr, m.rho);
+    if (path == kRowInside)
+        scatter<S, SWAPPED, PERIODIC, kRowInside>(a, g, fr, gr, m.rho);
+    else if (!PERIODIC && path == kAllInside)
+        scatter<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr, m.rho);
     else
-        scatter<S, SWAPPED, PERIODIC, false>(a, g, fr, gr, m.rho);
+        scatter<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fr, gr, m.rho);
     return {m, g.iy};
 }
 
@@ -1029,18 +1108,39 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
 // 128 threads per SM (64 registers, no spills): B200, 256^3, 24.6 GLUPS
 // FP16S and 23.7 BF16S, against 20.7 and 21.3 for the one-thread-per-node
 // kernel at 4 blocks.
+//
+// With OBS, the kernel also reduces the observables of the state it reads
+// into one row of kObsTerms FP64 sums per block (a.obs_rows), as step_kernel
+// does: half 0 of each warp pair brings its 32 nodes' moments, half 1 zeros.
 constexpr int kSplitBlocks = 8;
-template <class S, bool SWAPPED, bool PERIODIC>
+template <class S, bool SWAPPED, bool PERIODIC, bool OBS = false>
 __global__ void __launch_bounds__(128, kSplitBlocks) step16_split_kernel(const StepArgs<S> a) {
     __shared__ float xch[2][2][5][32];   // [warp pair][half][moment][lane]
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int pair = warp >> 1;
     const uint32_t n = blockIdx.x * 64u + (uint32_t)(pair * 32 + lane);
     const bool valid = n < a.nodes;
+    NodeOut<float> o;
     if ((warp & 1) == 0)
-        split_update<0, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+        o = split_update<0, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
     else
-        split_update<1, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+        o = split_update<1, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+    if constexpr (OBS) {
+        const bool mine = valid && (warp & 1) == 0;
+        double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+        bool bad = false;
+        if (mine) {
+            const double ux = o.m.ux, uy = o.m.uy, uz = o.m.uz, phi = o.m.phi;
+            d[0] = uy * phi;
+            d[1] = ux * ux + uy * uy + uz * uz;
+            d[2] = ux;
+            d[3] = uy;
+            d[4] = uz;
+            d[5] = phi;
+            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)o.m.rho);
+        }
+        block_obs_row<128>(d, mine ? o.iy : 0, mine, bad, a.ly, a.obs_rows + (size_t)blockIdx.x * kObsTerms);
+    }
 }
 
 }  // namespace lbm

@@ -1,10 +1,10 @@
 """Observables reduced inside the step kernels (lbm_step_observed) against
 the separate reduction (lbm_get_observables) of the same states.
 
-For FP64 and FP32 storage the step kernels reduce the moments they compute
-anyway, in FP64, in another order than lbm_get_observables: FP64 rounding
-apart.  For 16-bit storage lbm_step_observed runs the separate reduction
-before each step (faster there), so the results are the same."""
+The step kernels reduce the moments they compute anyway, in FP64, in another
+order than lbm_get_observables: FP64 rounding apart.  For 16-bit BGK cases
+lbm_get_observables forms each node's moments exactly as the split step
+kernel does (the same loads and partial sums), so this holds there too."""
 import numpy as np
 import pytest
 
