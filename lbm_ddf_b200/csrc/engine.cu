@@ -464,6 +464,9 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
 // nodes per block there, 128 in step_kernel.
 bool split_step(const lbm_case *c) { return interleaved(c) && c->collision == LBM_COLLISION_BGK; }
 int step_blocks(const lbm_case *c) { return (int)grid_for(c->nodes, split_step(c) ? 64 : kStepThreads); }
+// rows of observables sums an observed step writes: one per warp of the node
+// kernel, one per warp pair of the 16-bit split kernel
+int obs_rows_of(const lbm_case *c) { return step_blocks(c) * (split_step(c) ? 2 : kStepThreads / 32); }
 
 template <class S, bool SW, bool PER, bool OBS = false>
 void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
@@ -482,7 +485,7 @@ void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
 }
 
 // One node-kernel step that also writes the observables of the state it
-// reads as per-block rows into a.obs_rows.
+// reads as per-warp rows into a.obs_rows.
 template <class S> void launch_step_observed(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
     const bool per = c->p.sides == LBM_SIDES_PERIODIC;
     if (c->swapped) {
@@ -914,13 +917,13 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
     if (nsteps == 0) return LBM_OK;
     DeviceGuard dg(c->p.device);
     cudaStream_t st = (cudaStream_t)stream;
-    // one row per step-kernel block: room for the 64-node blocks of the
-    // 16-bit BGK kernel, whichever kernel the case uses now
-    const int rows = step_blocks(c);
+    // one row per warp of the node kernel (per warp pair of the 16-bit BGK
+    // kernel): room for the most rows, whichever kernel the case uses now
+    const int rows = obs_rows_of(c);
     const int parts = (rows + kRowChunk - 1) / kRowChunk;
-    const int max_rows = (int)grid_for(c->nodes, 64);
+    const int max_rows = (int)grid_for(c->nodes, kStepThreads) * (kStepThreads / 32);
     const int max_parts = (max_rows + kRowChunk - 1) / kRowChunk;
-    if (!c->obs_rows) {   // per-block rows, then the chunk partials behind them
+    if (!c->obs_rows) {   // per-warp rows, then the chunk partials behind them
         CUDA_TRY(cudaMalloc(&c->obs_rows, (size_t)(max_rows + max_parts) * kObs * sizeof(double)));
     }
     if (nsteps > c->obs_series_cap) {

@@ -28,7 +28,7 @@ struct lbm_case {
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
     int obs_blocks = 0;
-    double *obs_rows = nullptr;          // lbm_step_observed: per-block rows + chunk partials
+    double *obs_rows = nullptr;          // lbm_step_observed: per-warp rows + chunk partials
     lbm_observables *obs_series = nullptr;
     int obs_series_cap = 0;
 };

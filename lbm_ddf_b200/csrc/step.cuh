@@ -108,7 +108,7 @@ template <class S> struct StepArgs {
         return reinterpret_cast<typename Pack16<SS>::T *>(pairs_st[k / 9])[(uint32_t)(k % 9) * pair_row +
                                                                            (uint32_t)j];
     }
-    double *obs_rows;  // fused observables: one row of kObsTerms sums per block (else unused)
+    double *obs_rows;  // fused observables: one row of kObsTerms sums per warp (else unused)
     S *pairs[3];       // 16-bit storage: rows 0, 9 and 18 of the (f, g) pair array
     S *pairs_st[3];    // the same, for the stores (see fs)
     uint32_t pair_row; // pairs per row (the padded node count)
@@ -616,18 +616,18 @@ __device__ __forceinline__ void add_obs_terms(double (&acc)[kObsTerms], const Mo
         acc[12] += 1.0;
 }
 
-// The block's sums of the kObsTerms terms of its nodes into row[0 ..
-// kObsTerms); every thread of the block calls it, `valid` false for threads
-// past the last node.  Each thread brings its node's six dense terms (0-5)
-// and plane; per warp, the six are summed by butterflies; the plane terms
-// are the warp's phi sum when all its nodes lie in one plane (rows of a
-// multiple of 32 nodes), else butterflies too; the non-finite count is a
-// ballot.  Then the warps' sums are added in warp order.
-template <int BLOCK>
-__device__ __forceinline__ void block_obs_row(const double (&d)[6], int iy, bool valid, bool bad, int ly,
-                                              double *__restrict__ row) {
-    __shared__ double red[kObsTerms][BLOCK / 32];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+// The warp's sums of the kObsTerms terms of its nodes into row[0 ..
+// kObsTerms); all 32 lanes call it, `valid` false for lanes without a node.
+// Each lane brings its node's six dense terms (0-5) and plane; the six are
+// summed by butterflies; the plane terms are the warp's phi sum when all its
+// nodes lie in one plane (rows of a multiple of 32 nodes), else butterflies
+// too; the non-finite count is a ballot.  One row per warp and no block
+// barrier: a warp that finishes its nodes early leaves at once instead of
+// waiting for the block's slowest warp (in a closed box, the warps holding
+// an x-wall node take the longer update).
+__device__ __forceinline__ void warp_obs_row(const double (&d)[6], int iy, bool valid, bool bad, int ly,
+                                             double *__restrict__ row) {
+    const int lane = threadIdx.x & 31;
     double w[kObsTerms];
 #pragma unroll
     for (int k = 0; k < 6; k++) w[k] = warp_sum(d[k]);
@@ -643,13 +643,7 @@ __device__ __forceinline__ void block_obs_row(const double (&d)[6], int iy, bool
     w[12] = (double)__popc(__ballot_sync(0xffffffffu, valid && bad));
     if (lane == 0) {
 #pragma unroll
-        for (int k = 0; k < kObsTerms; k++) red[k][warp] = w[k];
-    }
-    __syncthreads();
-    if (threadIdx.x < kObsTerms) {
-        double t = 0.0;
-        for (int v = 0; v < BLOCK / 32; v++) t += red[threadIdx.x][v];
-        row[threadIdx.x] = t;
+        for (int k = 0; k < kObsTerms; k++) row[k] = w[k];
     }
 }
 
@@ -957,14 +951,39 @@ __device__ __forceinline__ void pair_barrier(int pair) {
         asm volatile("barrier.sync 2, 64;\n" ::: "memory");
 }
 
+// Receives a node's moments as soon as a node update (update_node,
+// split_update) has formed them, before the collision and the scatter.
+struct NoMomentSink {
+    template <class R> __device__ __forceinline__ void operator()(const Moments<R> &) const {}
+};
+
+// Parks a node's moments (ux, uy, uz, phi, rho) in shared memory, STRIDE
+// elements apart, so a kernel that reduces them after the update does not
+// hold them in registers through the collision and the scatter (in the FP64
+// kernel, at its register limit, that cost a third of the swapped-layout
+// step in a closed box).  T holds the moments exactly (T = double, or float
+// for float moments).  Volatile, so the compiler does not forward the stores
+// to the loads.
+template <class T, int STRIDE> struct SharedMomentSink {
+    volatile T *p;
+    template <class R> __device__ __forceinline__ void operator()(const Moments<R> &m) const {
+        static_assert(sizeof(T) >= sizeof(R), "the parked moments must hold the update's exactly");
+        p[0] = (T)m.ux;
+        p[STRIDE] = (T)m.uy;
+        p[2 * STRIDE] = (T)m.uz;
+        p[3 * STRIDE] = (T)m.phi;
+        p[4 * STRIDE] = (T)m.rho;
+    }
+};
+
 // Half H of the update of node n (valid: n is a node); xch is the warp
 // pair's exchange area [half][moment][lane].  Both warps of a pair call it
 // once, valid or not, and pass the barrier once.
 // Returns the node's moments (those of the state it read) and plane; they
 // are meaningful for valid nodes only.
-template <int H, class S, bool SWAPPED, bool PERIODIC, class A>
+template <int H, class S, bool SWAPPED, bool PERIODIC, class A, class Sink = NoMomentSink>
 __device__ __forceinline__ NodeOut<float> split_update(const A &a, uint32_t n, bool valid, float (&xch)[2][5][32],
-                                                       int lane, int pair) {
+                                                       int lane, int pair, const Sink &sink = Sink()) {
     float2 fg[Q];
     float p[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
     Node g{};
@@ -997,6 +1016,7 @@ __device__ __forceinline__ NodeOut<float> split_update(const A &a, uint32_t n, b
     m.uz = tot[3];
     m.phi = tot[4] + s0;
     if (a.use_phi_fix) m.phi = a.phi_fix;
+    sink(m);
     const bool fold = SWAPPED && (path == kAllInside || (PERIODIC && path == kRowInside));
     collide_half<H>(fg, m, a.omega_f, a.omega_g, a.force_fac, a.gb, a.t0, s0, fold ? (float)a.t_dy : 0.f);
     if (H == 0) a.phip[n] = m.phi;
@@ -1040,10 +1060,13 @@ __device__ __forceinline__ Moments<float> split_moments(const A &a, const Node &
     return m;
 }
 
-template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A>
-__device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a, uint32_t n) {
+template <class S, bool SWAPPED, bool PERIODIC, int COLL = LBM_COLLISION_BGK, class A, class Sink = NoMomentSink>
+__device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a, uint32_t n,
+                                                                     const Sink &sink = Sink()) {
     if constexpr (sizeof(S) == 2 && COLL == LBM_COLLISION_BGK) {
-        return update_node_norm<S, SWAPPED, PERIODIC>(a, n);
+        const auto o = update_node_norm<S, SWAPPED, PERIODIC>(a, n);
+        sink(o.m);
+        return o;
     }
     using R = typename Codec<S>::R;
     const Node g = make_node<PERIODIC>(a, n);
@@ -1060,6 +1083,7 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     else
         gather<S, SWAPPED, kNoneInside>(a, g, fr, gr);
     const Moments<R> m = node_moments<S>(a, fr, gr, n);
+    sink(m);
     collide<S, COLL>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
     if (path == kRowInside)
@@ -1073,8 +1097,8 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
 
 // One time step.  With OBS, the kernel also reduces the observables of the
 // state it reads — the moments every node update computes anyway — into one
-// row of kObsTerms FP64 sums per block (a.obs_rows), at no extra read of the
-// populations.
+// row of kObsTerms FP64 sums per warp (a.obs_rows, row 4 b + w for warp w of
+// block b), at no extra read of the populations.
 template <class S, bool SWAPPED, bool PERIODIC, int COLL, bool OBS = false>
 __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(const StepArgs<S> a) {
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1082,24 +1106,25 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
         if (n >= a.nodes) return;
         update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
     } else {
+        __shared__ double parked[5][128];   // ux, uy, uz, phi, rho per thread
         // the terms of add_obs_terms: uy*phi, |u|^2, ux, uy, uz, phi
         double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         int iy = 0;
         bool bad = false;
         const bool valid = n < a.nodes;
         if (valid) {
-            const auto o = update_node<S, SWAPPED, PERIODIC, COLL>(a, n);
-            const double ux = o.m.ux, uy = o.m.uy, uz = o.m.uz, phi = o.m.phi;
+            volatile double *mine = &parked[0][threadIdx.x];
+            iy = update_node<S, SWAPPED, PERIODIC, COLL>(a, n, SharedMomentSink<double, 128>{mine}).iy;
+            const double ux = mine[0], uy = mine[128], uz = mine[256], phi = mine[384], rho = mine[512];
             d[0] = uy * phi;
             d[1] = ux * ux + uy * uy + uz * uz;
             d[2] = ux;
             d[3] = uy;
             d[4] = uz;
             d[5] = phi;
-            iy = o.iy;
-            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)o.m.rho);
+            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite(rho);
         }
-        block_obs_row<128>(d, iy, valid, bad, a.ly, a.obs_rows + (size_t)blockIdx.x * kObsTerms);
+        warp_obs_row(d, iy, valid, bad, a.ly, a.obs_rows + ((size_t)blockIdx.x * 4 + (threadIdx.x >> 5)) * kObsTerms);
     }
 }
 
@@ -1110,8 +1135,11 @@ __global__ void __launch_bounds__(128, StepOccupancy<S>::value) step_kernel(cons
 // kernel at 4 blocks.
 //
 // With OBS, the kernel also reduces the observables of the state it reads
-// into one row of kObsTerms FP64 sums per block (a.obs_rows), as step_kernel
-// does: half 0 of each warp pair brings its 32 nodes' moments, half 1 zeros.
+// into one row of kObsTerms FP64 sums per warp pair (a.obs_rows, row 2 b + p
+// for pair p of block b): half 0 parks its 32 nodes' moments in shared memory
+// when it forms them and reduces them after its update; half 1 leaves when
+// its update is done.  (Splitting the reduction between the halves measured
+// slower: both then form the terms.)
 constexpr int kSplitBlocks = 8;
 template <class S, bool SWAPPED, bool PERIODIC, bool OBS = false>
 __global__ void __launch_bounds__(128, kSplitBlocks) step16_split_kernel(const StepArgs<S> a) {
@@ -1120,26 +1148,33 @@ __global__ void __launch_bounds__(128, kSplitBlocks) step16_split_kernel(const S
     const int pair = warp >> 1;
     const uint32_t n = blockIdx.x * 64u + (uint32_t)(pair * 32 + lane);
     const bool valid = n < a.nodes;
-    NodeOut<float> o;
-    if ((warp & 1) == 0)
-        o = split_update<0, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
-    else
-        o = split_update<1, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
-    if constexpr (OBS) {
-        const bool mine = valid && (warp & 1) == 0;
+    if constexpr (!OBS) {
+        if ((warp & 1) == 0)
+            split_update<0, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+        else
+            split_update<1, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+    } else {
+        __shared__ float parked[2][5][32];   // [warp pair][ux, uy, uz, phi, rho][lane]
+        if (warp & 1) {
+            split_update<1, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair);
+            return;
+        }
+        volatile float *mine = &parked[pair][0][lane];
+        const int iy = split_update<0, S, SWAPPED, PERIODIC>(a, n, valid, xch[pair], lane, pair,
+                                                             SharedMomentSink<float, 32>{mine}).iy;
         double d[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
         bool bad = false;
-        if (mine) {
-            const double ux = o.m.ux, uy = o.m.uy, uz = o.m.uz, phi = o.m.phi;
+        if (valid) {
+            const double ux = mine[0], uy = mine[32], uz = mine[64], phi = mine[96], rho = mine[128];
             d[0] = uy * phi;
             d[1] = ux * ux + uy * uy + uz * uz;
             d[2] = ux;
             d[3] = uy;
             d[4] = uz;
             d[5] = phi;
-            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite((double)o.m.rho);
+            bad = !isfinite(ux) || !isfinite(uy) || !isfinite(uz) || !isfinite(phi) || !isfinite(rho);
         }
-        block_obs_row<128>(d, mine ? o.iy : 0, mine, bad, a.ly, a.obs_rows + (size_t)blockIdx.x * kObsTerms);
+        warp_obs_row(d, iy, valid, bad, a.ly, a.obs_rows + ((size_t)blockIdx.x * 2 + pair) * kObsTerms);
     }
 }
 
