@@ -125,12 +125,14 @@ struct ObsConsts {
 // lanes) and forms the observables: Nu_bulk of src/output.cu:228-233;
 // Nu_top/bottom of :236-256 written with plane sums,
 // <(3T0 - 4T1 + T2)/2> = (3<T0> - 4<T1> + <T2>)/2.  Launch: kObs warps.
-__global__ void __launch_bounds__(32 * kObs) obs_finalize(const double *__restrict__ partial, int nblocks,
-                                                          ObsConsts c, lbm_observables *__restrict__ out) {
+// The body of obs_finalize, for a block of kObs warps; `partial` is read
+// through L2 (it may have been written by other blocks of the same launch).
+__device__ __forceinline__ void finalize_observables(const double *__restrict__ partial, int nblocks,
+                                                     const ObsConsts &c, lbm_observables *__restrict__ out) {
     __shared__ double tot[kObs];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double s = 0.0;
-    for (int b = lane; b < nblocks; b += 32) s += partial[(size_t)b * kObs + w];
+    for (int b = lane; b < nblocks; b += 32) s += __ldcg(partial + (size_t)b * kObs + w);
     s = warp_sum(s);
     if (lane == 0) tot[w] = s;
     __syncthreads();
@@ -156,20 +158,44 @@ __global__ void __launch_bounds__(32 * kObs) obs_finalize(const double *__restri
     }
 }
 
-// The per-block rows a fused step kernel wrote, summed in blocks of
-// kRowChunk rows into one partial row each (warp w sums term w, lane l the
-// rows l, l + 32, ... of the chunk, then a butterfly over the lanes): a
-// fixed order, so the result is deterministic.  Launch: kObs warps.
+__global__ void __launch_bounds__(32 * kObs) obs_finalize(const double *__restrict__ partial, int nblocks,
+                                                          ObsConsts c, lbm_observables *__restrict__ out) {
+    finalize_observables(partial, nblocks, c, out);
+}
+
+// The per-warp rows a fused step kernel wrote, summed in blocks of
+// kRowChunk rows into one partial row each, then (by the block that finishes
+// last) the partial rows into the observables, as obs_finalize forms them.
+// Thread t of a block reads the chunk's words t, t + 32 kObs, ...: coalesced,
+// and all of term t % kObs, rows t / kObs + 32 i; the 32 threads of a term
+// are then added by a butterfly in row order.  A fixed order, so the result
+// is deterministic.  `done` counts the blocks that have written their
+// partial row; the last one resets it to 0 for the next launch.  Launch: kObs
+// warps per block.
 constexpr int kRowChunk = 1024;
 __global__ void __launch_bounds__(32 * kObs) obs_rows_reduce(const double *__restrict__ rows, int nrows,
-                                                             double *__restrict__ partial) {
-    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+                                                             double *__restrict__ partial,
+                                                             unsigned *__restrict__ done, ObsConsts c,
+                                                             lbm_observables *__restrict__ out) {
+    __shared__ double red[32 * kObs];
+    __shared__ bool last;
+    const int t = threadIdx.x, w = t >> 5, lane = t & 31;
     const int r0 = blockIdx.x * kRowChunk;
-    const int r1 = min(nrows, r0 + kRowChunk);
+    const int words = (min(nrows, r0 + kRowChunk) - r0) * kObs;
+    const double *chunk = rows + (size_t)r0 * kObs;
     double s = 0.0;
-    for (int r = r0 + lane; r < r1; r += 32) s += rows[(size_t)r * kObs + w];
-    s = warp_sum(s);
-    if (lane == 0) partial[(size_t)blockIdx.x * kObs + w] = s;
+    for (int e = t; e < words; e += 32 * kObs) s += chunk[e];
+    red[t] = s;
+    __syncthreads();
+    const double v = warp_sum(red[lane * kObs + w]);   // term w, rows lane + 32 i
+    if (lane == 0) partial[(size_t)blockIdx.x * kObs + w] = v;
+    __threadfence();
+    __syncthreads();
+    if (t == 0) last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    finalize_observables(partial, gridDim.x, c, out);
+    if (t == 0) *done = 0u;
 }
 
 // Vertical profile, src/output.cu:336-368: one block per xz plane iy.
@@ -923,8 +949,10 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
     const int parts = (rows + kRowChunk - 1) / kRowChunk;
     const int max_rows = (int)grid_for(c->nodes, kStepThreads) * (kStepThreads / 32);
     const int max_parts = (max_rows + kRowChunk - 1) / kRowChunk;
-    if (!c->obs_rows) {   // per-warp rows, then the chunk partials behind them
-        CUDA_TRY(cudaMalloc(&c->obs_rows, (size_t)(max_rows + max_parts) * kObs * sizeof(double)));
+    if (!c->obs_rows) {   // per-warp rows, the chunk partials, the count of chunks done
+        const size_t bytes = (size_t)(max_rows + max_parts) * kObs * sizeof(double);
+        CUDA_TRY(cudaMalloc(&c->obs_rows, bytes + sizeof(double)));
+        CUDA_TRY(cudaMemsetAsync((char *)c->obs_rows + bytes, 0, sizeof(double), st));
     }
     if (nsteps > c->obs_series_cap) {
         if (c->obs_series) {
@@ -937,6 +965,7 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
         c->obs_series_cap = nsteps;
     }
     double *partial = c->obs_rows + (size_t)max_rows * kObs;
+    unsigned *done = (unsigned *)(partial + (size_t)max_parts * kObs);
     rc = with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         StepArgs<S> a = make_args<S>(c);
@@ -951,8 +980,7 @@ static int step_observed(lbm_case *c, int32_t nsteps, lbm_observables *out, void
         for (int s = 0; s < nsteps; s++) {
             k.step = c->step + s;   // the state this step starts from
             launch_step_observed<S>(c, a, st);
-            obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial);
-            obs_finalize<<<1, 32 * kObs, 0, st>>>(partial, parts, k, c->obs_series + s);
+            obs_rows_reduce<<<parts, 32 * kObs, 0, st>>>(c->obs_rows, rows, partial, done, k, c->obs_series + s);
             c->swapped = !c->swapped;
             c->rest_phi = false;
             a.use_phi_fix = 0;
