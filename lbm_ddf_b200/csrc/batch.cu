@@ -63,9 +63,10 @@ template <class S> struct BatchCase {
     // in 32 bits (a member has 27 ps elem_stride < 2^32 elements per
     // array): one multiply-add per access and no 64-bit row addresses held
     // in registers
-    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const {
-        return (which ? g : f)[((uint32_t)k * ps + (uint32_t)j) * elem_stride<S>()];
+    template <class I> __device__ __forceinline__ const S *ldp(int which, int k, I j) const {
+        return (which ? g : f) + ((uint32_t)k * ps + (uint32_t)j) * elem_stride<S>();
     }
+    template <class I> __device__ __forceinline__ S ld(int which, int k, I j) const { return *ldp(which, k, j); }
     template <class I> __device__ __forceinline__ S &st(int which, int k, I j) const {
         return (which ? g_st : f_st)[((uint32_t)k * ps + (uint32_t)j) * elem_stride<S>()];
     }
