@@ -142,7 +142,11 @@ int lbm_init_conduction(lbm_case *c, uint64_t seed, double amplitude, void *stre
  * g_i = w_i T and carried previous temperature = T, with T[idx] (idx =
  * (iz*LY + iy)*LX + ix, the reference's node order) copied from `temperature`
  * — host (pinned or pageable) or device memory, in the carried-temperature
- * type: double for F64 storage, float otherwise.  With the T that
+ * type: double for F64 storage, float otherwise.  Memory the device can read
+ * (its own, or page-locked host memory from cudaHostAlloc) is read by the
+ * initialising kernel itself, the PCIe transfer overlapping the writes of the
+ * populations; other memory is copied in first.  Returns with the state
+ * written.  With the T that
  * lbm_init_conduction forms it gives that call's state bit for bit in F64
  * storage.  The reference starts from its rest state (init_arrays) or a
  * restart file only. */

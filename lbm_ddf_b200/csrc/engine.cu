@@ -329,7 +329,7 @@ __device__ __forceinline__ uint64_t splitmix64(uint64_t x) {
 // T + amplitude*(2u - 1), so every build gives the same bits.
 template <class S>
 __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, double amplitude, double t_hot,
-                            double t_cold) {
+                            double t_cold, const typename Codec<S>::P *temperature) {
     using C = Codec<S>;
     using R = typename C::R;
     const uint32_t n = blockIdx.x * blockDim.x + threadIdx.x;
@@ -346,7 +346,7 @@ __global__ void init_kernel(const StepArgs<S> a, int mode, uint64_t seed_key, do
         t = __dsub_rn(t_hot, __ddiv_rn(__dmul_rn(__dsub_rn(t_hot, t_cold), (double)iy), __dsub_rn((double)a.ly, 1.0)));
         t = __dadd_rn(t, __dmul_rn(amplitude, __dsub_rn(__dmul_rn(2.0, u), 1.0)));
     } else if (mode == 2) {
-        t = (double)a.phip[n];
+        t = (double)temperature[n];
     }
     Unroll<0, Q>::run([&](auto kk) {
         constexpr int K = decltype(kk)::value;
@@ -693,7 +693,10 @@ int lbm_destroy(lbm_case *c) {
     return LBM_OK;
 }
 
-static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, void *stream) {
+// mode 0: rest state; 1: seeded conduction state; 2: from `temperature`
+// (one carried-temperature value per node, readable by the device).
+static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, void *stream,
+                       const void *temperature = nullptr) {
     int rc = check_mutable(c, false);
     if (rc) return rc;
     DeviceGuard dg(c->p.device);
@@ -707,7 +710,8 @@ static int init_common(lbm_case *c, int mode, uint64_t seed, double amplitude, v
     rc = with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const StepArgs<S> a = make_args<S>(c);
-        init_kernel<S><<<grid_for(c->nodes, 256), 256, 0, st>>>(a, mode, key, amplitude, c->p.t_hot, c->p.t_cold);
+        init_kernel<S><<<grid_for(c->nodes, 256), 256, 0, st>>>(
+            a, mode, key, amplitude, c->p.t_hot, c->p.t_cold, (const typename Codec<S>::P *)temperature);
         return LBM_OK;
     });
     if (rc) return rc;
@@ -732,9 +736,25 @@ int lbm_init_temperature(lbm_case *c, const void *temperature, void *stream) {
     if (rc) return rc;
     if (!temperature) return fail(LBM_ERR_ARG, "temperature is NULL");
     DeviceGuard dg(c->p.device);
+    // Memory this device can read (its own, or page-locked host memory
+    // mapped into its address space, as cudaHostAlloc gives under unified
+    // addressing): the init kernel reads the field itself, host memory over
+    // PCIe while it writes the populations to HBM, so the transfer and the
+    // initialisation overlap.  Anything else (pageable memory, another
+    // device's): copied into the carried-temperature array first.
+    const void *direct = nullptr;
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, temperature) == cudaSuccess) {
+        if ((at.type == cudaMemoryTypeDevice && at.device == c->p.device) || at.type == cudaMemoryTypeHost ||
+            at.type == cudaMemoryTypeManaged)
+            direct = at.devicePointer;
+    } else {
+        cudaGetLastError();   // an unknown pointer is not an error here: it is copied
+    }
+    if (direct) return init_common(c, 2, 0, 0.0, stream, direct);
     const size_t bytes = (size_t)c->nodes * (c->p.storage == LBM_STORE_F64 ? sizeof(double) : sizeof(float));
     CUDA_TRY(cudaMemcpyAsync(c->phip, temperature, bytes, cudaMemcpyDefault, (cudaStream_t)stream));
-    return init_common(c, 2, 0, 0.0, stream);
+    return init_common(c, 2, 0, 0.0, stream, c->phip);
 }
 
 int lbm_load_ref_state(lbm_case *c, const double *rho, const double *ux, const double *uy, const double *uz,

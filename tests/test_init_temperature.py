@@ -97,12 +97,15 @@ def test_reduced_precision_temperature_start(gpu, storage, tol, periodic):
 
 
 @pytest.mark.gpu
-def test_temperature_from_pinned_and_device_tensors(gpu):
+@pytest.mark.parametrize("storage,dtype", [("f32", np.float32), ("f64", np.float64), ("f16s", np.float32)])
+def test_temperature_from_pinned_and_device_tensors(gpu, storage, dtype):
+    """Pageable host memory is copied in first; page-locked host memory and
+    device memory are read by the init kernel itself: the same state."""
     import torch
 
     lbm = gpu
-    p = _params(lbm, "f32", True)
-    t = lbm.conduction_temperature(LX, LY, LZ, SEED, AMP, dtype=np.float32)
+    p = _params(lbm, storage, False)
+    t = lbm.conduction_temperature(LX, LY, LZ, SEED, AMP, dtype=dtype)
     ref = _run(lbm, p, lambda c: c.init_temperature(t), 5)[1]
     pinned = torch.from_numpy(t).pin_memory()
     dev = torch.from_numpy(t).cuda()
