@@ -591,6 +591,35 @@ template <class S> cudaError_t launch_step(const lbm_case *c, const StepArgs<S> 
         }                                                                                 \
     } while (0)
 
+// Launches obs_kernel over case c's state (layout and sides as c says) into
+// `partial` and returns the blocks it ran: at most `cap` (the partial rows
+// there are) and at most the blocks `sms` SMs hold at once, so that the
+// grid-stride loop runs in one wave (8 blocks per SM asked of a kernel that
+// fits 5 would run a second, partly idle wave).
+template <class S, bool SW, bool PER> int obs_resident() {
+    static const int resident = [] {
+        int n = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, obs_kernel<S, SW, PER>, kObsThreads, 0) !=
+                cudaSuccess ||
+            n <= 0) {
+            cudaGetLastError();
+            n = 1;
+        }
+        return n;
+    }();
+    return resident;
+}
+template <class S>
+int launch_obs(const lbm_case *c, const StepArgs<S> &a, double *partial, int cap, int sms, int split,
+               cudaStream_t st) {
+    const bool per = c->p.sides == LBM_SIDES_PERIODIC;
+    const int resident = c->swapped ? (per ? obs_resident<S, true, true>() : obs_resident<S, true, false>())
+                                    : (per ? obs_resident<S, false, true>() : obs_resident<S, false, false>());
+    const int blocks = std::max(1, std::min(cap, sms * resident));
+    LBM_DISPATCH_LAYOUT(c, obs_kernel, blocks, kObsThreads, st, a, partial, split);
+    return blocks;
+}
+
 int check_case(const lbm_case *c, bool need_state) {
     if (!c) return fail(LBM_ERR_ARG, "case is NULL");
     if (need_state && !c->initialised) return fail(LBM_ERR_STATE, "case has no state yet (init or load first)");
@@ -650,7 +679,8 @@ int lbm_create(const lbm_params *p, lbm_case **out) {
     c->nodes = (int64_t)p->lx * p->ly * p->lz;
     c->ps = round_up(c->nodes, 128);
     DeviceGuard dg(p->device);
-    c->obs_blocks = obs_blocks_for(c->nodes, sm_count_of(p->device));
+    c->sms = sm_count_of(p->device);
+    c->obs_blocks = obs_blocks_for(c->nodes, c->sms);
     const size_t sb = store_bytes(p->storage);
     const size_t pop_bytes = (size_t)Q * (size_t)c->ps * sb;
     const size_t carry_bytes = (size_t)c->ps * (p->storage == LBM_STORE_F64 ? 8 : 4);
@@ -897,7 +927,7 @@ int lbm_internal::enqueue_observables(const lbm_case *c, lbm_observables *dst, c
     return with_storage(c, [&](auto tag) {
         using S = std::remove_pointer_t<decltype(tag)>;
         const StepArgs<S> a = make_args<S>(c);
-        LBM_DISPATCH_LAYOUT(c, obs_kernel, c->obs_blocks, kObsThreads, st, a, c->partial, split_step(c) ? 1 : 0);
+        const int blocks = launch_obs<S>(c, a, c->partial, c->obs_blocks, c->sms, split_step(c) ? 1 : 0, st);
         ObsConsts k;
         k.nodes = (double)c->nodes;
         k.plane = (double)c->p.lx * (double)c->p.lz;
@@ -906,7 +936,7 @@ int lbm_internal::enqueue_observables(const lbm_case *c, lbm_observables *dst, c
         k.dT = c->p.t_hot - c->p.t_cold;
         k.visc = c->d.visc;
         k.step = c->step;
-        obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, c->obs_blocks, k, dst);
+        obs_finalize<<<1, 32 * kObs, 0, st>>>(c->partial, blocks, k, dst);
         return LBM_OK;
     });
 }
@@ -1202,7 +1232,7 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
     int sms = 0;
     rc = noalloc_scratch(p->device, &scratch, &sms);
     if (rc) return rc;
-    const int blocks = obs_blocks_for(nodes, sms);   // <= kObsMaxBlocks = the array's rows
+    const int cap = obs_blocks_for(nodes, sms);   // <= kObsMaxBlocks = the array's rows
     lbm_case view;               // a stack view of the caller's buffers; owns nothing
     view.p = *p;
     derive(p, &view.d);
@@ -1220,7 +1250,7 @@ int lbm_observables_noalloc(const lbm_params *p, const void *f, const void *g, c
         const StepArgs<S> a = make_args<S>(&view);
         const lbm_case *c = &view;
         // 16-bit storage: the moments as the BGK step kernel forms them
-        LBM_DISPATCH_LAYOUT(c, obs_kernel, blocks, kObsThreads, st, a, scratch, interleaved(c) ? 1 : 0);
+        const int blocks = launch_obs<S>(c, a, scratch, cap, sms, interleaved(c) ? 1 : 0, st);
         ObsConsts k;
         k.nodes = (double)nodes;
         k.plane = (double)p->lx * (double)p->lz;

@@ -27,7 +27,8 @@ struct lbm_case {
     uint32_t debug_extra_tx = 0;         // lbm_debug_row_wait_extra_bytes (0: off)
     double *partial = nullptr;           // obs partial sums
     lbm_observables *d_obs = nullptr;    // reduced observables (device)
-    int obs_blocks = 0;
+    int obs_blocks = 0;                  // partial rows (most reduction blocks)
+    int sms = 148;                       // SM count of the case's device
     double *obs_rows = nullptr;          // lbm_step_observed: per-warp rows + chunk partials
     lbm_observables *obs_series = nullptr;
     int obs_series_cap = 0;

@@ -29,8 +29,11 @@ def _close(got, want, rel, ab):
 @pytest.mark.parametrize("storage", ["f64", "f32", "f16s", "bf16s"])
 @pytest.mark.parametrize("periodic", [True, False])
 @pytest.mark.parametrize("collision", ["bgk", "regularized"])
-def test_step_observed_matches_get_observables(lbm, storage, periodic, collision):
-    p = lbm.make_params(24, 20, 16, rayleigh=1e6, storage=storage,
+@pytest.mark.parametrize("shape", [(24, 20, 16), (64, 12, 10)])
+def test_step_observed_matches_get_observables(lbm, storage, periodic, collision, shape):
+    """Rows of 24 nodes: warps straddle rows and planes; rows of 64: whole
+    warps, a closed box's inner warps on the path without boundary tests."""
+    p = lbm.make_params(*shape, rayleigh=1e6, storage=storage,
                         sides=lbm.SIDES_PERIODIC if periodic else lbm.SIDES_WALL)
     with lbm.Case(p) as a, lbm.Case(p) as b:
         for c in (a, b):
