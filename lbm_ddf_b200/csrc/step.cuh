@@ -177,12 +177,19 @@ __device__ __forceinline__ bool inside(const Node &g) {
 //                at the x walls of a closed box;
 //   kAllInside:  all of them (a closed box's rows whose warp holds no x-wall
 //                node: with LX a multiple of 32, all but the first and last
-//                warp of a row).
-constexpr int kNoneInside = 0, kRowInside = 1, kAllInside = 2;
+//                warp of a row);
+//   kRowLoWall, kRowHiWall: as kRowInside, in a closed box's warp whose
+//                x-wall nodes, if any, all lie at x = 0 (Lo) or all at
+//                x = LX-1 (Hi): only the x neighbour on that side is tested
+//                (the first and last warp of a row, with LX a multiple of 32
+//                and at least 64).
+constexpr int kNoneInside = 0, kRowInside = 1, kAllInside = 2, kRowLoWall = 3, kRowHiWall = 4;
 template <int INTERIOR, int DX, int DY, int DZ>
 __device__ __forceinline__ bool inside_t(const Node &g) {
     if constexpr (INTERIOR == kAllInside) return true;
     else if constexpr (INTERIOR == kRowInside) return DX < 0 ? g.vxm : DX > 0 ? g.vxp : true;
+    else if constexpr (INTERIOR == kRowLoWall) return DX < 0 ? g.vxm : true;
+    else if constexpr (INTERIOR == kRowHiWall) return DX > 0 ? g.vxp : true;
     else return inside<DX, DY, DZ>(g);
 }
 // whether every neighbour of a node taking this path is inside (so the
@@ -207,6 +214,19 @@ template <bool PERIODIC> __device__ __forceinline__ int node_path(const Node &g)
     if (!yz_interior<PERIODIC>(g)) return kNoneInside;
     if constexpr (!PERIODIC) {
         if (__all_sync(__activemask(), g.vxm && g.vxp)) return kAllInside;
+    }
+    return kRowInside;
+}
+// node_path, with a closed box's warps at one x wall told apart (kRowLoWall,
+// kRowHiWall), for updates that take those paths.
+template <bool PERIODIC> __device__ __forceinline__ int node_path_x(const Node &g) {
+    if (!yz_interior<PERIODIC>(g)) return kNoneInside;
+    if constexpr (!PERIODIC) {
+        const unsigned active = __activemask();
+        const bool lo_in = __all_sync(active, g.vxm), hi_in = __all_sync(active, g.vxp);
+        if (lo_in && hi_in) return kAllInside;
+        if (hi_in) return kRowLoWall;
+        if (lo_in) return kRowHiWall;
     }
     return kRowInside;
 }
@@ -1079,14 +1099,20 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     const Node g = make_node<PERIODIC>(a, n);
     R fr[Q], gr[Q];
     // Rows away from the plates (and, in a closed box, from the z walls)
-    // need no y or z boundary tests, and a closed box's warps with no x-wall
-    // node none at all; the path is uniform over a warp whenever LX is a
-    // multiple of 32.
-    const int path = node_path<PERIODIC>(g);
+    // need no y or z boundary tests, a closed box's warps with no x-wall
+    // node none at all, and in the swapped layout (the one whose accesses
+    // depend on them) the warps at one x wall tests on that side only; the
+    // path is uniform over a warp whenever LX is a multiple of 32.
+    constexpr bool kOneWall = SWAPPED && !PERIODIC;
+    const int path = kOneWall ? node_path_x<PERIODIC>(g) : node_path<PERIODIC>(g);
     if (path == kRowInside)
         gather<S, SWAPPED, kRowInside>(a, g, fr, gr);
     else if (!PERIODIC && path == kAllInside)
         gather<S, SWAPPED, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr);
+    else if (kOneWall && path == kRowLoWall)
+        gather<S, SWAPPED, kOneWall ? kRowLoWall : kRowInside>(a, g, fr, gr);
+    else if (kOneWall && path == kRowHiWall)
+        gather<S, SWAPPED, kOneWall ? kRowHiWall : kRowInside>(a, g, fr, gr);
     else
         gather<S, SWAPPED, kNoneInside>(a, g, fr, gr);
     const Moments<R> m = node_moments<S>(a, fr, gr, n);
@@ -1097,6 +1123,10 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
         scatter<S, SWAPPED, PERIODIC, kRowInside>(a, g, fr, gr, m.rho);
     else if (!PERIODIC && path == kAllInside)
         scatter<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr, m.rho);
+    else if (kOneWall && path == kRowLoWall)
+        scatter<S, SWAPPED, PERIODIC, kOneWall ? kRowLoWall : kRowInside>(a, g, fr, gr, m.rho);
+    else if (kOneWall && path == kRowHiWall)
+        scatter<S, SWAPPED, PERIODIC, kOneWall ? kRowHiWall : kRowInside>(a, g, fr, gr, m.rho);
     else
         scatter<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fr, gr, m.rho);
     return {m, g.iy};
