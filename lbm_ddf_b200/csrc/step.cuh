@@ -218,7 +218,9 @@ template <bool PERIODIC> __device__ __forceinline__ int node_path(const Node &g)
     return kRowInside;
 }
 // node_path, with a closed box's warps at one x wall told apart (kRowLoWall,
-// kRowHiWall), for updates that take those paths.
+// kRowHiWall), for updates that take those paths (the node kernel's swapped
+// layout; in the 16-bit split kernel the two extra paths measured 12% slower
+// on the swapped closed-box step).
 template <bool PERIODIC> __device__ __forceinline__ int node_path_x(const Node &g) {
     if (!yz_interior<PERIODIC>(g)) return kNoneInside;
     if constexpr (!PERIODIC) {
