@@ -117,7 +117,10 @@ int lbm_abi_version(void);
 int lbm_derive(const lbm_params *p, lbm_derived *out);
 
 /* Device bytes a case with these parameters holds (populations, carried
- * temperature, reduction scratch), for admission against a memory budget. */
+ * temperature, reduction scratch), for admission against a memory budget.
+ * The first lbm_step_observed call adds the rows of its in-kernel reduction
+ * (13 doubles per 32 nodes, under 4 bytes per node) and one lbm_observables
+ * per step of the longest call made. */
 int lbm_case_bytes(const lbm_params *p, uint64_t *bytes);
 
 /* Allocates a case on p->device (replaces the cudaMalloc calls of
