@@ -1,7 +1,7 @@
 // bulk.cuh — thin wrappers over the sm_90+/sm_100a bulk asynchronous copy
-// (TMA, untiled) and mbarrier PTX used by the row-staged step.  Only
-// non-multicast forms: every copy moves one contiguous row between this
-// GPU's global memory and the issuing CTA's shared memory.
+// (TMA, untiled) and mbarrier PTX used by the row-staged step.  Every copy
+// moves one contiguous row between this GPU's global memory and the issuing
+// CTA's own shared memory (no copy fans out to other CTAs of a cluster).
 //
 // Rules the callers keep: global and shared addresses 16-byte aligned, sizes
 // a multiple of 16 bytes; shared memory written by ordinary stores is made

@@ -1,5 +1,5 @@
 // rowstep.cuh — the fused step with whole x-rows staged through shared memory
-// by bulk asynchronous copies (TMA, untiled, no multicast).
+// by bulk asynchronous copies (TMA, untiled, each into its own CTA).
 //
 // Same update as step_kernel (step.cuh), same AA layouts, same results; only
 // the data movement differs.  One block owns one x-row of the grid (LX
