@@ -210,9 +210,13 @@ template <bool PERIODIC> __device__ __forceinline__ bool yz_interior(const Node 
 // kRowInside for rows whose y and z neighbours are inside, kAllInside for
 // those of a closed box when no active lane of the warp lies at an x wall
 // (decided over the warp, so a warp takes one path), else kNoneInside.
-template <bool PERIODIC> __device__ __forceinline__ int node_path(const Node &g) {
+// In the natural layout every access is at the node itself, so kAllInside
+// would compile to kRowInside's code again: with SWAPPED false it is not
+// returned, which keeps a third copy of the update out of the kernel (in the
+// issue-bound 16-bit split kernel a larger body measured slower).
+template <bool PERIODIC, bool SWAPPED = true> __device__ __forceinline__ int node_path(const Node &g) {
     if (!yz_interior<PERIODIC>(g)) return kNoneInside;
-    if constexpr (!PERIODIC) {
+    if constexpr (!PERIODIC && SWAPPED) {
         if (__all_sync(__activemask(), g.vxm && g.vxp)) return kAllInside;
     }
     return kRowInside;
@@ -815,10 +819,10 @@ template <class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t n) {
     const Node g = make_node<PERIODIC>(a, n);
     float2 fg[Q];
-    const int path = node_path<PERIODIC>(g);
+    const int path = node_path<PERIODIC, SWAPPED>(g);
     if (path == kRowInside)
         gather_norm<S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
-    else if (!PERIODIC && path == kAllInside)
+    else if (SWAPPED && !PERIODIC && path == kAllInside)
         gather_norm<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
     else
         gather_norm<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
@@ -830,7 +834,7 @@ __device__ __forceinline__ NodeOut<float> update_node_norm(const A &a, uint32_t 
     a.phip[n] = m.phi;
     if (path == kRowInside)
         scatter_norm<S, SWAPPED, PERIODIC, kRowInside>(a, g, fg, m.rho, s0);
-    else if (!PERIODIC && path == kAllInside)
+    else if (SWAPPED && !PERIODIC && path == kAllInside)
         scatter_norm<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg, m.rho, s0);
     else
         scatter_norm<S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg, m.rho, s0);
@@ -1021,10 +1025,10 @@ __device__ __forceinline__ NodeOut<float> split_update(const A &a, uint32_t n, b
     if (valid) {
         phip = a.phip[n];   // before the barrier: half 0 overwrites it after
         g = make_node<PERIODIC>(a, n);
-        path = node_path<PERIODIC>(g);
+        path = node_path<PERIODIC, SWAPPED>(g);
         if (path == kRowInside)
             gather_half<H, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
-        else if (!PERIODIC && path == kAllInside)
+        else if (SWAPPED && !PERIODIC && path == kAllInside)
             gather_half<H, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
         else
             gather_half<H, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg);
@@ -1051,7 +1055,7 @@ __device__ __forceinline__ NodeOut<float> split_update(const A &a, uint32_t n, b
     if (H == 0) a.phip[n] = m.phi;
     if (path == kRowInside)
         scatter_half<H, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg, m.rho, s0);
-    else if (!PERIODIC && path == kAllInside)
+    else if (SWAPPED && !PERIODIC && path == kAllInside)
         scatter_half<H, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg, m.rho, s0);
     else
         scatter_half<H, S, SWAPPED, PERIODIC, kNoneInside>(a, g, fg, m.rho, s0);
@@ -1066,11 +1070,11 @@ template <class S, bool SWAPPED, bool PERIODIC, class A>
 __device__ __forceinline__ Moments<float> split_moments(const A &a, const Node &g) {
     float2 fg[Q];
     float p0[5], p1[5];
-    const int path = node_path<PERIODIC>(g);
+    const int path = node_path<PERIODIC, SWAPPED>(g);
     if (path == kRowInside) {
         gather_half<0, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
         gather_half<1, S, SWAPPED, PERIODIC, kRowInside>(a, g, fg);
-    } else if (!PERIODIC && path == kAllInside) {
+    } else if (SWAPPED && !PERIODIC && path == kAllInside) {
         gather_half<0, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
         gather_half<1, S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fg);
     } else {
@@ -1106,10 +1110,10 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     // depend on them) the warps at one x wall tests on that side only; the
     // path is uniform over a warp whenever LX is a multiple of 32.
     constexpr bool kOneWall = SWAPPED && !PERIODIC;
-    const int path = kOneWall ? node_path_x<PERIODIC>(g) : node_path<PERIODIC>(g);
+    const int path = kOneWall ? node_path_x<PERIODIC>(g) : node_path<PERIODIC, SWAPPED>(g);
     if (path == kRowInside)
         gather<S, SWAPPED, kRowInside>(a, g, fr, gr);
-    else if (!PERIODIC && path == kAllInside)
+    else if (SWAPPED && !PERIODIC && path == kAllInside)
         gather<S, SWAPPED, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr);
     else if (kOneWall && path == kRowLoWall)
         gather<S, SWAPPED, kOneWall ? kRowLoWall : kRowInside>(a, g, fr, gr);
@@ -1123,7 +1127,7 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     a.phip[n] = (typename Codec<S>::P)m.phi;
     if (path == kRowInside)
         scatter<S, SWAPPED, PERIODIC, kRowInside>(a, g, fr, gr, m.rho);
-    else if (!PERIODIC && path == kAllInside)
+    else if (SWAPPED && !PERIODIC && path == kAllInside)
         scatter<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr, m.rho);
     else if (kOneWall && path == kRowLoWall)
         scatter<S, SWAPPED, PERIODIC, kOneWall ? kRowLoWall : kRowInside>(a, g, fr, gr, m.rho);
