@@ -233,6 +233,7 @@ template <bool PERIODIC> __device__ __forceinline__ int node_path_x(const Node &
         if (lo_in && hi_in) return kAllInside;
         if (hi_in) return kRowLoWall;
         if (lo_in) return kRowHiWall;
+        return kNoneInside;   // a warp at both x walls (rows shorter than 64 or not whole warps)
     }
     return kRowInside;
 }
@@ -1111,7 +1112,7 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     // path is uniform over a warp whenever LX is a multiple of 32.
     constexpr bool kOneWall = SWAPPED && !PERIODIC;
     const int path = kOneWall ? node_path_x<PERIODIC>(g) : node_path<PERIODIC, SWAPPED>(g);
-    if (path == kRowInside)
+    if (!kOneWall && path == kRowInside)
         gather<S, SWAPPED, kRowInside>(a, g, fr, gr);
     else if (SWAPPED && !PERIODIC && path == kAllInside)
         gather<S, SWAPPED, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr);
@@ -1125,7 +1126,7 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     sink(m);
     collide<S, COLL>(fr, gr, m, a);
     a.phip[n] = (typename Codec<S>::P)m.phi;
-    if (path == kRowInside)
+    if (!kOneWall && path == kRowInside)
         scatter<S, SWAPPED, PERIODIC, kRowInside>(a, g, fr, gr, m.rho);
     else if (SWAPPED && !PERIODIC && path == kAllInside)
         scatter<S, SWAPPED, PERIODIC, PERIODIC ? kRowInside : kAllInside>(a, g, fr, gr, m.rho);
