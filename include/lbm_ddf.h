@@ -107,6 +107,11 @@ typedef struct lbm_observables {
     int32_t reserved;
 } lbm_observables;
 
+/* One simulation case: its state and reduction buffers on p->device.  Calls
+ * on one case come from one host thread at a time, and its GPU work runs in
+ * the order of the streams it is given: work of one case enqueued on two
+ * streams that may run at once races (the state, and the reduction rows of
+ * lbm_step_observed, are the case's own).  Different cases are independent. */
 typedef struct lbm_case lbm_case;
 
 /* Message of the last failing call on this host thread ("" if none). */
