@@ -1108,7 +1108,7 @@ __device__ __forceinline__ NodeOut<typename Codec<S>::R> update_node(const A &a,
     // Rows away from the plates (and, in a closed box, from the z walls)
     // need no y or z boundary tests, a closed box's warps with no x-wall
     // node none at all, and in the swapped layout (the one whose accesses
-    // depend on them) the warps at one x wall tests on that side only; the
+    // depend on them) the warps at one x wall test that side only; the
     // path is uniform over a warp whenever LX is a multiple of 32.
     constexpr bool kOneWall = SWAPPED && !PERIODIC;
     const int path = kOneWall ? node_path_x<PERIODIC>(g) : node_path<PERIODIC, SWAPPED>(g);
