@@ -503,11 +503,17 @@ void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
             return;
         }
     }
-    const unsigned grid = grid_for(c->nodes, kStepThreads);
+    // FP32 plain steps in blocks of two warps: a block keeps its SM slot
+    // until its slowest warp is done, and smaller blocks waste less of it
+    // (B200, 256^3: natural layout -1.8%, closed-box swapped -3.6%); FP64
+    // measured 3% slower so, and the observed steps keep four warps (their
+    // rows are numbered by four warps per block)
+    constexpr int threads = (!OBS && std::is_same<S, float>::value) ? 64 : kStepThreads;
+    const unsigned grid = grid_for(c->nodes, threads);
     if (c->collision == LBM_COLLISION_REGULARIZED)
-        step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED, OBS><<<grid, kStepThreads, 0, st>>>(a);
+        step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED, OBS><<<grid, threads, 0, st>>>(a);
     else
-        step_kernel<S, SW, PER, LBM_COLLISION_BGK, OBS><<<grid, kStepThreads, 0, st>>>(a);
+        step_kernel<S, SW, PER, LBM_COLLISION_BGK, OBS><<<grid, threads, 0, st>>>(a);
 }
 
 // One node-kernel step that also writes the observables of the state it
