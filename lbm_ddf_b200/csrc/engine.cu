@@ -489,10 +489,16 @@ template <class Fn> int with_storage(const lbm_case *c, Fn &&fn) {
 // Whether the case steps on step16_split_kernel (16-bit storage, BGK): 64
 // nodes per block there, 128 in step_kernel.
 bool split_step(const lbm_case *c) { return interleaved(c) && c->collision == LBM_COLLISION_BGK; }
-int step_blocks(const lbm_case *c) { return (int)grid_for(c->nodes, split_step(c) ? 64 : kStepThreads); }
+int step_blocks(const lbm_case *c) {
+    if (split_step(c)) return (int)grid_for(c->nodes, 64);
+    return (int)grid_for(c->nodes, c->p.storage == LBM_STORE_F32 ? node_threads<float>() : kStepThreads);
+}
 // rows of observables sums an observed step writes: one per warp of the node
 // kernel, one per warp pair of the 16-bit split kernel
-int obs_rows_of(const lbm_case *c) { return step_blocks(c) * (split_step(c) ? 2 : kStepThreads / 32); }
+int obs_rows_of(const lbm_case *c) {
+    if (split_step(c)) return step_blocks(c) * 2;
+    return step_blocks(c) * ((c->p.storage == LBM_STORE_F32 ? node_threads<float>() : kStepThreads) / 32);
+}
 
 template <class S, bool SW, bool PER, bool OBS = false>
 void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
@@ -503,12 +509,7 @@ void launch_step_t(const lbm_case *c, const StepArgs<S> &a, cudaStream_t st) {
             return;
         }
     }
-    // FP32 plain steps in blocks of two warps: a block keeps its SM slot
-    // until its slowest warp is done, and smaller blocks waste less of it
-    // (B200, 256^3: natural layout -1.8%, closed-box swapped -3.6%); FP64
-    // measured 3% slower so, and the observed steps keep four warps (their
-    // rows are numbered by four warps per block)
-    constexpr int threads = (!OBS && std::is_same<S, float>::value) ? 64 : kStepThreads;
+    constexpr int threads = node_threads<S>();
     const unsigned grid = grid_for(c->nodes, threads);
     if (c->collision == LBM_COLLISION_REGULARIZED)
         step_kernel<S, SW, PER, LBM_COLLISION_REGULARIZED, OBS><<<grid, threads, 0, st>>>(a);
